@@ -1,0 +1,211 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures from the reference's own code.
+
+Run in a checkout where the FastCorticalWiring reference is importable
+(default /root/reference, or --reference PATH). The GPU box never runs this:
+its outputs are committed next to it as small .npz files.
+
+Reference code run here, unmodified:
+  * fastcw_lean.ConsistentBatchHeatEngine (factor="scipy")  -- heat-method distances
+  * fastcw_lean.fused_normalized_divergence                 -- divergence of X
+  * lean_geometry.per_source_geometry / area_at / perimeter_at / solve_radius / field_health
+  * core_analysis.FastCorticalWiringAnalysis.compute_all_wiring_costs, with an
+    engine registered into distance_engines.ENGINE_REGISTRY that wraps the
+    heat engine (the same hook lean_testkit.install_stubs uses)
+  * lean_testkit icosphere/bumpy meshes + euclid stub fields (geometry KATs)
+
+Fixtures:
+  golden_heat_L4.npz      seeded folded L4 mesh, distances/heat/divergence for 8 sources,
+                          per-source FP64 geometry, health, MSD/boundary, and the
+                          float32 arrays the analysis loop writes (incl. sample CSR)
+  golden_metrics_L5.npz   same analysis outputs on a seeded folded L5 mesh (16 sources)
+  golden_geometry_kat.npz lean geometry on euclid-stub and non-Lipschitz fields (L4 bumpy),
+                          area/perimeter at fixed radii, per_source_geometry, NaN rules
+"""
+
+import argparse
+import contextlib
+import io
+import os
+import sys
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def _ref_modules(path):
+    sys.path.insert(0, path)
+    import lean_testkit as tk  # noqa: E402
+
+    tk.install_stubs()
+    import core_analysis as ca  # noqa: E402
+    import distance_engines as de  # noqa: E402
+    import fastcw_lean as fl  # noqa: E402
+    import lean_geometry as lg  # noqa: E402
+
+    class ConsistentHeatReference(de.BaseDistanceEngine):
+        """The reference's own batched heat engine, one source per call."""
+
+        def __init__(self, vertices, faces, **kw):
+            super().__init__(vertices, faces, **kw)
+            L = float(self.engine_kwargs.get("diffusion_length_mm", 0.7))
+            h = lg.mean_edge_length(self.vertices, self.faces)
+            self._eng = fl.ConsistentBatchHeatEngine(self.vertices, self.faces, t_coef=(L / h) ** 2,
+                                                     factor="scipy")
+
+        @property
+        def name(self):
+            return "consistent_heat_reference"
+
+        def compute_distance(self, s):
+            return self._eng.compute_distance(int(s))
+
+    de.ENGINE_REGISTRY["consistent_heat_reference"] = ConsistentHeatReference
+    return ca, de, fl, lg, tk
+
+
+SCALES = [0.002, 0.00267988, 0.00359088, 0.00481157, 0.00644721, 0.00863888,
+          0.01157558, 0.01551059, 0.02078326, 0.02784833, 0.03731509, 0.05]
+
+
+def _analysis_fixture(ca, lg, fl, mesh, n_sources, with_stages):
+    with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()):
+        an = ca.FastCorticalWiringAnalysis(mesh.vertices, mesh.faces, mesh.cortex_mask,
+                                           engine_type="consistent_heat_reference")
+    order = np.asarray(an._bfs_order)
+    pick = order[np.linspace(0, order.size - 1, n_sources).astype(int)]
+    subset = an.sub_to_orig[pick]
+    with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()), \
+            warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        an.compute_all_wiring_costs(scale=SCALES, vertex_subset=subset, n_samples_between_scales=3)
+    out = dict(
+        V=mesh.vertices, F=mesh.faces, mask=mesh.cortex_mask, level=mesh.level, seed=mesh.seed,
+        jitter=mesh.jitter, scales=np.asarray(SCALES), sources_sub=pick.astype(np.int64),
+        sources_orig=subset.astype(np.int64), bfs_order=order.astype(np.int64),
+        boundary=an.boundary_indices.astype(np.int64), vertex_area=an.vertex_areas_sub,
+        health_h=an._health_h, bin_width=an._lean_width,
+        t=an.distance_engine._eng.t,
+    )
+    for k, v in an.get_metric_arrays().items():
+        out["f32_" + k] = v[subset]
+    out["field_flag"] = an.field_flag[subset]
+    indptr, rs, as_ = [0], [], []
+    for o in subset:
+        r, a = an.get_vertex_samples(int(o))
+        rs.append(r)
+        as_.append(a)
+        indptr.append(indptr[-1] + r.size)
+    out["sample_indptr"] = np.asarray(indptr, np.int64)
+    out["sample_r"] = np.concatenate(rs).astype(np.float32)
+    out["sample_a"] = np.concatenate(as_).astype(np.float32)
+    # FP64 per-stage values from the reference engine and lean geometry
+    eng = an.distance_engine._eng
+    phi = eng.compute_distance_batch(pick)
+    out["phi"] = phi
+    T = np.array(SCALES) * float(an.vertex_areas_sub.sum())
+    out["targets"] = T
+    fr = np.array([0.25, 0.5, 0.75])
+    nF = an.faces.shape[0]
+    bufs = (np.empty(nF), np.empty(nF, np.int32), np.empty(nF, np.int32))
+    R, P, ER, EA, NE, H = [], [], [], [], [], []
+    for j, s in enumerate(pick):
+        r, p, er, ea = np.empty(12), np.empty(12), np.empty(33), np.empty(33)
+        ne = lg.per_source_geometry(phi[j], an.faces, an._lean_area, an._lean_g11, an._lean_g12,
+                                    an._lean_g22, an._lean_width, T, fr, 1e-10, 60, *bufs, r, p, er, ea)
+        R.append(r)
+        P.append(p)
+        ER.append(er)
+        EA.append(ea)
+        NE.append(ne)
+        H.append(lg.field_health(phi[j], an.vertices, int(s), an._health_h))
+    out.update(radii=np.array(R), perim=np.array(P), extra_r=np.array(ER), extra_a=np.array(EA),
+               n_eval=np.array(NE), health=np.array([[h[0], h[1], float(h[2])] for h in H]))
+    if with_stages:
+        src2 = pick[:3]
+        rhs = np.zeros((eng.n_vertices, src2.size))
+        rhs[src2, np.arange(src2.size)] = 1.0
+        u = np.ascontiguousarray(eng._heat.solve(rhs))
+        div = np.empty_like(u)
+        fl.fused_normalized_divergence(u, eng.F, eng.area, eng.gb0, eng.gb1, eng.gb2, div)
+        out.update(stage_sources=src2.astype(np.int64), stage_u=u, stage_div=div)
+    return out
+
+
+def _geometry_kat(ca, lg, tk):
+    V, F = tk.icosphere(4)
+    with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()):
+        an = ca.FastCorticalWiringAnalysis(tk.bumpy(V), F, np.ones(len(V), bool), engine_type="euclid_stub")
+    Vs, Fs = an.vertices, an.faces
+    nF = len(Fs)
+    area, g11, g12, g22 = lg.precompute_face_metric(Vs, Fs)
+    w = lg.default_bin_width(Vs, Fs)
+    bufs = (np.empty(nF), np.empty(nF, np.int32), np.empty(nF, np.int32))
+    rng = np.random.default_rng(1)
+    fields = [an._compute_geodesic_distances_from_subvertex(int(s)) for s in rng.choice(len(Vs), 3, replace=False)]
+    d = an._compute_geodesic_distances_from_subvertex(7).copy()
+    bad = rng.choice(len(d), len(d) // 50, replace=False)
+    d[bad] += rng.uniform(0, 15, bad.size)
+    fields.append(d)
+    fields = np.array(fields)
+    radii = np.array([rng.uniform(0.5, np.nanmax(f) * 0.8, 12) for f in fields])
+    A, DA, P, NL = [], [], [], []
+    for f, rr in zip(fields, radii):
+        nb, ptr, pre, nl = lg.build_distance_buckets(f, Fs, area, w, *bufs)
+        a_row, da_row, p_row = [], [], []
+        for r in rr:
+            a, da = lg.area_at(r, f, Fs, area, w, nb, ptr, pre, bufs[1], bufs[0], bufs[2], nl)
+            a_row.append(a)
+            da_row.append(da)
+            p_row.append(lg.perimeter_at(r, f, Fs, area, g11, g12, g22, w, nb, ptr, bufs[1], bufs[0], bufs[2], nl))
+        A.append(a_row)
+        DA.append(da_row)
+        P.append(p_row)
+        NL.append(nl)
+    T = np.array(SCALES) * float(an.vertex_areas_sub.sum())
+    fr = np.array([0.25, 0.5, 0.75])
+    G = []
+    for f in (fields[0], fields[3]):
+        ro, po, er, ea = np.empty(12), np.empty(12), np.empty(33), np.empty(33)
+        n = lg.per_source_geometry(f, Fs, area, g11, g12, g22, w, T, fr, 1e-12, 60, *bufs, ro, po, er, ea)
+        G.append((ro, po, er, ea, n))
+    f = fields[3]
+    nb, ptr, pre, nl = lg.build_distance_buckets(f, Fs, area, w, *bufs)
+    a_nan, _ = lg.area_at(np.nan, f, Fs, area, w, nb, ptr, pre, bufs[1], bufs[0], bufs[2], nl)
+    r_nan, _ = lg.solve_radius(np.nan, f, Fs, area, w, nb, ptr, pre, bufs[1], bufs[0], bufs[2], nl, 1e-12, 60)
+    r_big, _ = lg.solve_radius(pre[nb] * 2, f, Fs, area, w, nb, ptr, pre, bufs[1], bufs[0], bufs[2], nl, 1e-12, 60)
+    r_zero, _ = lg.solve_radius(0.0, f, Fs, area, w, nb, ptr, pre, bufs[1], bufs[0], bufs[2], nl, 1e-12, 60)
+    return dict(
+        V=Vs, F=Fs, fields=fields, radii_eval=radii, area_eval=np.array(A), darea_eval=np.array(DA),
+        perim_eval=np.array(P), n_long=np.array(NL), bin_width=w, targets=T, fracs=fr,
+        geo_radii=np.array([g[0] for g in G]), geo_perim=np.array([g[1] for g in G]),
+        geo_extra_r=np.array([g[2] for g in G]), geo_extra_a=np.array([g[3] for g in G]),
+        geo_n_eval=np.array([g[4] for g in G]), total_area=pre[nb],
+        nan_area=a_nan, nan_radius=r_nan, big_radius=r_big, zero_radius=r_zero,
+    )
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    sys.path.insert(0, REPO)
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    ca, de, fl, lg, tk = _ref_modules(args.reference)
+    l4 = folded_icosphere(4, seed=11, jitter=0.2)
+    np.savez_compressed(os.path.join(HERE, "golden_heat_L4.npz"), **_analysis_fixture(ca, lg, fl, l4, 8, True))
+    l5 = folded_icosphere(5, seed=5)
+    fx = _analysis_fixture(ca, lg, fl, l5, 16, False)
+    fx.pop("phi")  # large; the L5 fixture pins outputs, not fields
+    np.savez_compressed(os.path.join(HERE, "golden_metrics_L5.npz"), **fx)
+    np.savez_compressed(os.path.join(HERE, "golden_geometry_kat.npz"), **_geometry_kat(ca, lg, tk))
+    for n in ("golden_heat_L4.npz", "golden_metrics_L5.npz", "golden_geometry_kat.npz"):
+        print(n, os.path.getsize(os.path.join(HERE, n)))
+
+
+if __name__ == "__main__":
+    main()
