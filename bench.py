@@ -1,0 +1,480 @@
+#!/usr/bin/env python3
+"""All-sources heat-method throughput on B200 (sources/s), FastCorticalWiring hot path.
+
+Workload: the order-7 folded icosphere (163,842 vertices, 10% medial-wall cap
+removed -> 147,458 cortical sources), t = (0.7 mm)^2, the runner's 12 area
+fractions, 3 samples between scales (45 radii per source). A step is one batch
+of `--batch` sources (in BFS order, walking through all cortical sources):
+heat solve, normalised-gradient divergence, Poisson solve, shift, health,
+MSD, distance to boundary, 12 radii + perimeters, 33 samples.
+
+  python bench.py [--gpus N --steps K --warmup W]        # this engine
+  python bench.py --impl reference [...]                  # the CPU path, all host cores
+
+`value` is timed on the device (CUDA events, inputs resident in HBM, max over
+ranks); `e2e` runs the same steps through the host-buffer public API with the
+copies inside the timed region. Each rank holds a full replica of the mesh and
+its factors and processes its own slice of the sources (weak scaling).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "L5": dict(level=5, jitter=0.0), "L6": dict(level=6, jitter=0.2),
+    "L7": dict(level=7, jitter=0.0), "L8": dict(level=8, jitter=0.2),
+}
+METRIC = "sources/s @164k verts"
+N_BETWEEN = 3
+L2_BYTES = 126 * 1024 * 1024
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _mesh(workload, seed):
+    from fastcorticalwiring_b200 import mesh as M
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    cfg = WORKLOADS[workload]
+    m = folded_icosphere(cfg["level"], seed=seed, jitter=cfg["jitter"])
+    return m, M.prepare(m.vertices, m.faces, m.cortex_mask)
+
+
+# ---------------------------------------------------------------------------
+# CPU path: the oracle's per-source pipeline (the reference's algorithm)
+# ---------------------------------------------------------------------------
+def _cpu_source(ho, pm, targets, s):
+    import oracle
+
+    d = ho.distances([int(s)])[0]
+    return oracle.source_metrics(d, int(s), pm, targets)
+
+
+def _cpu_worker(workload, seed, sources, q):
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    import oracle
+    from fastcorticalwiring_b200 import mesh as M
+
+    _, pm = _mesh(workload, seed)
+    targets = pm.targets(M.RUNNER_SCALES)
+    ho = oracle.HeatOracle(pm.V, pm.F)
+    _cpu_source(ho, pm, targets, sources[0])  # warm caches
+    t0 = time.perf_counter()
+    for s in sources:
+        _cpu_source(ho, pm, targets, s)
+    q.put((len(sources), time.perf_counter() - t0))
+
+
+def _start_cpu_baseline(workload, seed, n):
+    from fastcorticalwiring_b200.meshgen import folded_icosphere  # noqa: F401  (import check only)
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    _, pm = _mesh(workload, seed)
+    bfs = pm.bfs
+    sources = [int(x) for x in bfs[np.linspace(0, bfs.size - 1, n).astype(int)]]
+    p = ctx.Process(target=_cpu_worker, args=(workload, seed, sources, q), daemon=True)
+    p.start()
+    return p, q, n
+
+
+def run_reference(args):
+    """CPU arm: the oracle's per-source pipeline on every host core (fork after the factorisation)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    import oracle
+    from fastcorticalwiring_b200 import mesh as M
+
+    _, pm = _mesh(args.workload, args.seed)
+    targets = pm.targets(M.RUNNER_SCALES)
+    t0 = time.perf_counter()
+    ho = oracle.HeatOracle(pm.V, pm.F)
+    factor_s = time.perf_counter() - t0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    per_step = args.ref_sources_per_core
+    bfs = pm.bfs
+    ctx = mp.get_context("fork")  # no GPU is touched in this arm
+
+    def step(i):
+        idx = np.linspace(0, bfs.size - 1, cores * per_step * (args.steps + args.warmup)).astype(int)
+        chunk = bfs[idx[i * cores * per_step:(i + 1) * cores * per_step]]
+        return [chunk[c::cores] for c in range(cores)]
+
+    global _REF_STATE
+    _REF_STATE = (ho, pm, targets)
+    times = []
+    with ctx.Pool(cores) as pool:
+        for i in range(args.warmup + args.steps):
+            parts = step(i)
+            t = time.perf_counter()
+            pool.map(_ref_task, parts)
+            if i >= args.warmup:
+                times.append(time.perf_counter() - t)
+    total = args.steps * cores * per_step
+    sec = sum(times)
+    value = total / sec
+    line = {
+        "metric": METRIC, "value": value, "unit": "sources/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": _config(args, pm),
+        "cpu_baseline": {"value": value, "unit": "sources/s", "cores": cores, "kind": "port",
+                         "sample": f"{per_step} sources per core per step, BFS-spaced over all "
+                                   f"{pm.n_vertices} sources; factorisation ({factor_s:.1f} s) excluded"},
+        "e2e": {"value": value, "unit": "sources/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+_REF_STATE = None
+
+
+def _ref_task(srcs):
+    ho, pm, targets = _REF_STATE
+    for s in srcs:
+        _cpu_source(ho, pm, targets, s)
+    return len(srcs)
+
+
+def _config(args, pm):
+    return {"workload": f"{args.workload} folded icosphere, {pm.n_vertices} cortical sources, "
+                        f"{pm.n_faces} faces, t=(0.7 mm)^2, 12 scales + {N_BETWEEN} samples between",
+            "batch_sources_per_step": args.batch, "block_k": args.block_k, "precision": args.precision,
+            "parallelism": f"replicas{args.gpus}", "l2": "inputs larger than L2 (n x K RHS blocks > 126 MB)"}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device), "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        out.update(sm_mhz=statistics.median(sm) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                   reasons=reasons, samples=len(rows))
+        return out
+
+
+def _stage_bytes(stage, n, nf, K, nnz_factor, precision, nreached_rows=None):
+    """Algorithmic bytes of one execution of a stage on a K-source block."""
+    b = 4 if precision == "mixed" else 8
+    if stage == "heat_bwd":
+        return nnz_factor * 8 + 2 * n * K * 8
+    if stage in ("poisson_fwd", "poisson_bwd"):
+        return nnz_factor * b + 2 * n * K * b
+    if stage == "divergence":
+        return n * K * 8 + n * K * b + nf * (3 * 4 + 4 * 4) + 3 * nf * 5
+    if stage == "shift":
+        return 2 * n * K * b
+    if stage == "vertex_stats":
+        return n * K * b + n * 32
+    if stage == "geometry":
+        return n * K * b + nf * (12 + 32)
+    if stage == "heat_fwd":
+        return nnz_factor * 8
+    return 0
+
+
+def run_gpu(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_sample > 0:
+        cpu = _start_cpu_baseline(args.workload, args.seed, args.cpu_sample)  # before any CUDA call
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from fastcorticalwiring_b200 import engine as E
+    from fastcorticalwiring_b200 import mesh as M
+
+    dev = local if world > 1 else args.device
+    torch.cuda.set_device(dev)
+    _, pm = _mesh(args.workload, args.seed)
+    targets = pm.targets(M.RUNNER_SCALES)
+    t0 = time.perf_counter()
+    eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k)
+    build_s = time.perf_counter() - t0
+    info = eng.info()
+
+    bfs = pm.bfs.astype(np.int32)
+    share = np.array_split(bfs, world)[rank]
+    B = args.batch
+    stride = E._lib.metrics_stride(12, N_BETWEEN)
+    src_dev = torch.from_numpy(share.copy()).to(f"cuda:{dev}")
+    out_dev = torch.empty((B, stride), dtype=torch.float64, device=f"cuda:{dev}")
+    stream = torch.cuda.Stream(device=dev)
+    nsteps_avail = max(1, share.size // B)
+
+    def step_slice(i):
+        j = i % nsteps_avail
+        return src_dev[j * B:(j + 1) * B]
+
+    def device_step(i, precision=args.precision):
+        eng.compute_metrics_device(step_slice(i), targets, N_BETWEEN, 1e-6, precision, out_dev,
+                                   stream.cuda_stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        device_step(i)
+    eng.synchronize(stream.cuda_stream)
+
+    # --- device-timed region ---
+    clocks = ClockSampler(dev)
+    clocks.start()
+    eng.profile(True)
+    torch.cuda.synchronize()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for i in range(args.steps):
+        device_step(args.warmup + i)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    stages, launches = eng.stage_times()
+    eng.profile(False)
+    clk = clocks.stop()
+    eng.synchronize(stream.cuda_stream)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_sources = B * args.steps * world
+    value = total_sources / (ms / 1e3)
+
+    # --- end to end through the host-buffer API (pinned host memory) ---
+    h_src = torch.from_numpy(share[:B * min(nsteps_avail, args.steps)].copy()).pin_memory().numpy()
+    h_out = torch.empty((B, stride), dtype=torch.float64).pin_memory().numpy()
+    lib = E._lib.load()
+    import ctypes
+
+    tgt = np.ascontiguousarray(targets)
+    prec = E._precision(args.precision)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        j = i % min(nsteps_avail, args.steps)
+        s = h_src[j * B:(j + 1) * B]
+        E._lib.check(lib.fcw_compute_metrics(eng.handle, ctypes.c_void_p(s.ctypes.data), s.size, prec,
+                                             E._lib.ptr(tgt), tgt.size, N_BETWEEN, 1e-6, E._lib.ptr(h_out)))
+    e2e_s = time.perf_counter() - t0
+    barrier()
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = total_sources / e2e_s
+
+    extra = {}
+    if rank == 0 and not args.quick:
+        extra = _fp64_forms_and_errors(eng, pm, targets, stream, args, dev)
+
+    if rank == 0:
+        hbm, peak_kind = _peaks()
+        nblocks = args.steps * ((B + args.block_k - 1) // args.block_k)
+        dom = max(stages, key=stages.get) if stages else None
+        roof = None
+        if dom and stages[dom] > 0:
+            per_block_s = stages[dom] / 1e3 / nblocks
+            byts = _stage_bytes(dom, pm.n_vertices, pm.n_faces, args.block_k, info["nnz_factor"], args.precision)
+            ach = byts / per_block_s / 1e9
+            roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                    "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
+                    "bytes_per_launch": byts, "launch": f"one {dom} stage on a {args.block_k}-source block"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 heat / f32 Poisson" if args.precision == "mixed" else "f64",
+            "data": "synthetic", "config": _config(args, pm),
+            "e2e": {"value": e2e, "unit": "sources/s", "h2d_bytes_per_step": B * 4 * world,
+                    "d2h_bytes_per_step": B * stride * 8 * world},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "stage_ms": {k: round(v, 3) for k, v in stages.items()},
+            "clocks": clk,
+            "engine": {"factor_ms": info["factor_ms"], "analyze_ms": info["analyze_ms"], "build_s": build_s,
+                       "n_supernodes": info["n_supernodes"], "n_levels": info["n_levels"],
+                       "nnz_factor": info["nnz_factor"], "device_bytes": info["device_bytes"]},
+        }
+        line.update(extra)
+        if cpu is not None:
+            p, q, n = cpu
+            try:
+                cnt, sec = q.get(timeout=args.cpu_timeout)
+                line["cpu_baseline"] = {"value": cnt / sec, "unit": "sources/s", "cores": 1, "kind": "port",
+                                        "sample": f"{cnt} BFS-spaced sources of the same mesh, one at a time, "
+                                                  "single thread, factorisation excluded"}
+            except Exception as exc:
+                line["cpu_baseline"] = {"value": None, "unit": "sources/s", "cores": 1, "kind": "port",
+                                        "sample": f"not finished: {exc!r}"}
+            p.join(timeout=5)
+        print(json.dumps(line))
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def _fp64_forms_and_errors(eng, pm, targets, stream, args, dev):
+    """The plain FP64 drop-in (one source per call) and the accuracy of the mixed form."""
+    import torch
+
+    from fastcorticalwiring_b200 import engine as E
+
+    bfs = pm.bfs.astype(np.int32)
+    # drop-in: one source per call, FP64, all metrics, host result
+    sample = bfs[np.linspace(0, bfs.size - 1, args.fp64_sample).astype(int)]
+    eng.compute_metrics(sample[:1], targets, N_BETWEEN, precision="fp64")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in sample:
+        eng.compute_metrics(np.array([s], np.int32), targets, N_BETWEEN, precision="fp64")
+    dropin = len(sample) / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for s in sample[:8]:
+        eng.compute_distance(int(s))
+    dist_only = 8 / (time.perf_counter() - t0)
+    # batched FP64 (same blocks as the headline, device timed)
+    B = min(args.batch, bfs.size)
+    src = torch.from_numpy(bfs[:B].copy()).to(f"cuda:{dev}")
+    stride = E._lib.metrics_stride(12, N_BETWEEN)
+    out = torch.empty((B, stride), dtype=torch.float64, device=f"cuda:{dev}")
+    eng.compute_metrics_device(src, targets, N_BETWEEN, 1e-6, "fp64", out, stream.cuda_stream)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(2):
+        eng.compute_metrics_device(src, targets, N_BETWEEN, 1e-6, "fp64", out, stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    fp64_batched = 2 * B / (ev0.elapsed_time(ev1) / 1e3)
+    # accuracy of the mixed form against the FP64 engine on one block
+    n = min(args.block_k, bfs.size)
+    chk = bfs[np.linspace(0, bfs.size - 1, n).astype(int)]
+    r64 = E.split_records(eng.compute_metrics(chk, targets, N_BETWEEN, precision="fp64"), 12, N_BETWEEN)
+    r32 = E.split_records(eng.compute_metrics(chk, targets, N_BETWEEN, precision="mixed"), 12, N_BETWEEN)
+    ok = ~(r64["bad"] | r32["bad"])
+
+    def rel(a, b):
+        a, b = a[ok], b[ok]
+        return float(np.nanmax(np.abs(a - b) / np.maximum(np.abs(b), 1e-300))) if a.size else None
+
+    d64 = eng.compute_distances(chk[:4], precision="fp64")
+    d32 = eng.compute_distances(chk[:4], precision="mixed")
+    return {
+        "fp64_forms": {"dropin_sources_per_s": dropin, "dropin_distance_only_per_s": dist_only,
+                       "batched_sources_per_s": fp64_batched, "sample": f"{len(sample)} sources one per call"},
+        "err_mixed_vs_fp64": {"radius": rel(r32["radii"], r64["radii"]), "perimeter": rel(r32["perim"], r64["perim"]),
+                              "msd_unweighted": rel(r32["msd_u"], r64["msd_u"]),
+                              "msd_weighted": rel(r32["msd_w"], r64["msd_w"]),
+                              "sample_area": rel(r32["extra_a"], r64["extra_a"]),
+                              "phi_max_abs_over_max": float(np.max(np.abs(d32 - d64)) / np.max(np.abs(d64))),
+                              "flag_mismatch": int(np.sum(r64["bad"] != r32["bad"])), "sources": int(n)},
+    }
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="L7")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--batch", type=int, default=2048, help="sources per step")
+    ap.add_argument("--block-k", type=int, default=256)
+    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--cpu-sample", type=int, default=24, help="sources timed on the CPU oracle (0 = skip)")
+    ap.add_argument("--cpu-timeout", type=float, default=600.0)
+    ap.add_argument("--fp64-sample", type=int, default=16)
+    ap.add_argument("--ref-sources-per-core", type=int, default=2)
+    ap.add_argument("--quick", action="store_true", help="skip the FP64 forms and the accuracy check")
+    args = ap.parse_args(argv)
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

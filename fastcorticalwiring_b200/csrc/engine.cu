@@ -1,0 +1,894 @@
+// Engine lifecycle, factorisation driver, the per-block pipeline and the C ABI.
+//
+// One engine = one cortical submesh on one GPU. Creation prepares the mesh on
+// the host, runs the symbolic analysis, uploads the structure and factors the
+// heat operator M + tL and the Poisson operator L + shift*M in FP64 on the
+// device (plus, for the mixed form, the Poisson operator grounded at the last
+// eliminated vertex, rounded to FP32). A block of K sources then runs:
+//   reach -> heat forward (delta RHS, pruned) -> heat backward -> divergence
+//   -> Poisson forward/backward -> shift + transpose -> vertex stats -> geometry
+// entirely on one stream.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fcw_b200.h"
+#include "fcw_internal.h"
+#include "kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define FCW_CUDA(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(FCW_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define FCW_TRY(expr)            \
+    do {                         \
+        int rc_ = (expr);        \
+        if (rc_ != FCW_OK) return rc_; \
+    } while (0)
+
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+__global__ void k_map_sources(int64_t n, const int32_t* __restrict__ sources, const int32_t* __restrict__ iperm,
+                              int32_t nv, int32_t K, int32_t* __restrict__ out, int* __restrict__ err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    int v = -1;
+    if (k < n) {
+        const int s = sources[k];
+        if (s >= 0 && s < nv) v = iperm[s];
+        else atomicOr(err, fcw::KERR_ARGS);
+    }
+    out[k] = v;
+}
+
+// d (k rows, caller vertex order) -> dT (K rows, elimination order); rows >= k are zero.
+__global__ void k_fields_in(int32_t n, int32_t k, int32_t K, const double* __restrict__ d,
+                            const int32_t* __restrict__ iperm, double* __restrict__ dT) {
+    const int64_t total = (int64_t)K * n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / n), i = (int)(e - (int64_t)r * n);
+        if (r < k) dT[(int64_t)r * n + iperm[i]] = d[e];
+    }
+}
+
+}  // namespace
+
+struct Workspace {
+    int32_t K = 0;
+    double* Bh = nullptr;
+    double* Bp64 = nullptr;
+    float* Bp32 = nullptr;
+    double* dT64 = nullptr;
+    float* dT32 = nullptr;
+    int32_t* src = nullptr;
+    uint8_t* reach = nullptr;
+    int32_t* band = nullptr;
+    int32_t* longf = nullptr;
+    double* out = nullptr;
+    int32_t out_stride = 0;
+};
+
+struct fcw_engine {
+    fcw_params prm{};
+    int device = 0;
+    fcw::MeshPrep mesh;
+    fcw::Symbolic sym;
+    double t_coef = 0.0, t = 0.0;
+    int32_t ground_new = -1;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocs;
+    int64_t bytes = 0;
+    fcw::DevPlan plan;
+    std::vector<int32_t> level_tiles;
+    double *val_h = nullptr, *inv_h = nullptr, *val_p = nullptr, *inv_p = nullptr;
+    float *val_g = nullptr, *inv_g = nullptr;
+    fcw::FaceData fd;
+    int32_t* iperm_d = nullptr;
+    int32_t* perm_d = nullptr;
+    double *coords_d = nullptr, *varea_d = nullptr, *farea_d = nullptr, *g11_d = nullptr, *g12_d = nullptr,
+           *g22_d = nullptr;
+    int32_t* boundary_d = nullptr;
+    int* err_d = nullptr;
+    Workspace ws;
+    double analyze_ms = 0.0, factor_ms = 0.0;
+    // stage timeline (CUDA events on the working stream), off unless enabled
+    bool prof_on = false;
+    std::vector<std::pair<int, cudaEvent_t>> marks;
+    std::vector<cudaEvent_t> event_pool;
+    double stage_ms[FCW_N_STAGES] = {0};
+    int64_t launches = 0;
+
+    template <typename T>
+    int dalloc(T** p, size_t count) {
+        *p = nullptr;
+        if (count == 0) count = 1;
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(FCW_E_NOMEM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed: " +
+                                         cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        bytes += (int64_t)(count * sizeof(T));
+        *p = static_cast<T*>(q);
+        return FCW_OK;
+    }
+    template <typename T>
+    int upload(T** p, const std::vector<T>& h) {
+        FCW_TRY(dalloc(p, h.size()));
+        if (!h.empty()) FCW_CUDA(cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return FCW_OK;
+    }
+    void release(void* p) {
+        for (size_t i = 0; i < allocs.size(); ++i)
+            if (allocs[i] == p) {
+                cudaFree(p);
+                allocs.erase(allocs.begin() + (long)i);
+                return;
+            }
+    }
+    ~fcw_engine() {
+        for (auto& m : marks) cudaEventDestroy(m.second);
+        for (cudaEvent_t ev : event_pool) cudaEventDestroy(ev);
+        for (void* p : allocs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int check_kernel_errors(fcw_engine* e, const char* where) {
+    int h = 0;
+    FCW_CUDA(cudaMemcpyAsync(&h, e->err_d, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    FCW_CUDA(cudaStreamSynchronize(e->stream));
+    if (h) {
+        FCW_CUDA(cudaMemsetAsync(e->err_d, 0, sizeof(int), e->stream));
+        std::string what;
+        if (h & fcw::KERR_NOT_SPD) what += " non-positive pivot (operator not SPD);";
+        if (h & fcw::KERR_HIST_OVERFLOW) what += " too many distance bins for one source;";
+        if (h & fcw::KERR_SCRATCH) what += " per-source face list overflow;";
+        if (h & fcw::KERR_ARGS) what += " invalid source index or launch arguments;";
+        return fail((h & fcw::KERR_ARGS) ? FCW_E_INVALID : FCW_E_NUMERIC, std::string(where) + ":" + what);
+    }
+    return FCW_OK;
+}
+
+// Record a stage boundary: the stage `stage` starts here (-1 = end of a block).
+void mark(fcw_engine* e, cudaStream_t st, int stage) {
+    if (!e->prof_on) return;
+    cudaEvent_t ev;
+    if (!e->event_pool.empty()) {
+        ev = e->event_pool.back();
+        e->event_pool.pop_back();
+    } else if (cudaEventCreate(&ev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaEventRecord(ev, st);
+    e->marks.push_back({stage, ev});
+}
+
+int collect_marks(fcw_engine* e) {
+    if (e->marks.empty()) return FCW_OK;
+    FCW_CUDA(cudaEventSynchronize(e->marks.back().second));
+    for (size_t j = 0; j + 1 < e->marks.size(); ++j) {
+        const int stg = e->marks[j].first;
+        if (stg < 0 || stg >= FCW_N_STAGES) continue;
+        float ms = 0.0f;
+        FCW_CUDA(cudaEventElapsedTime(&ms, e->marks[j].second, e->marks[j + 1].second));
+        e->stage_ms[stg] += ms;
+    }
+    for (auto& m : e->marks) e->event_pool.push_back(m.second);
+    e->marks.clear();
+    return FCW_OK;
+}
+
+int validate_params(const fcw_params* p) {
+    if (!p) return fail(FCW_E_INVALID, "params is NULL");
+    if (!std::isfinite(p->diffusion_length_mm) || p->diffusion_length_mm < 0.5)
+        return fail(FCW_E_INVALID, "diffusion_length_mm must be finite and at least 0.5 mm.");
+    if (!std::isfinite(p->poisson_shift) || p->poisson_shift < 0.0) return fail(FCW_E_INVALID, "invalid poisson_shift");
+    if (p->block_k < 32 || p->block_k % 32 != 0 || p->block_k > 4096)
+        return fail(FCW_E_INVALID, "block_k must be a multiple of 32 in [32, 4096]");
+    if (p->leaf_size < 1 || p->max_width < 1 || p->max_width > fcw::kMaxWidth)
+        return fail(FCW_E_INVALID, "max_width must be in [1, 64] and leaf_size >= 1");
+    if (p->relax < 1 || p->relax > p->max_width) return fail(FCW_E_INVALID, "relax must be in [1, max_width]");
+    if (p->refine_steps < 0 || p->refine_steps > 8) return fail(FCW_E_INVALID, "refine_steps must be in [0, 8]");
+    return FCW_OK;
+}
+
+// Values of A's lower entries in the symbolic analysis' order.
+enum class Op { Heat, Poisson, Grounded };
+std::vector<double> operator_values(const fcw_engine* e, Op op) {
+    const auto& S = e->sym;
+    const auto& m = e->mesh;
+    std::vector<double> v(S.nnz_lower_a);
+    const int32_t gold = e->ground_new >= 0 ? S.perm[e->ground_new] : -1;
+    for (int64_t q = 0; q < S.nnz_lower_a; ++q) {
+        const int64_t k = S.a_src[q];
+        const int32_t col = S.a_col[q], row = m.Li[k];
+        const bool diag = row == col;
+        const double L = m.Lx[k];
+        switch (op) {
+            case Op::Heat:  // M + t L (fastcw_lean.py:498)
+                v[q] = diag ? m.mass[col] + e->t * L : e->t * L;
+                break;
+            case Op::Poisson:  // L + shift M (fastcw_lean.py:500)
+                v[q] = diag ? L + e->prm.poisson_shift * m.mass[col] : L;
+                break;
+            case Op::Grounded:  // L with the ground vertex's row and column replaced by the identity
+                v[q] = (row == gold || col == gold) ? (diag ? 1.0 : 0.0) : L;
+                break;
+        }
+    }
+    return v;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// engine construction
+// ---------------------------------------------------------------------------
+namespace {
+
+int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, int64_t nf) {
+    std::string err;
+    double t0 = now_ms();
+    if (fcw::prepare_mesh(V, nv, F, nf, e->mesh, err)) return fail(FCW_E_INVALID, err);
+    e->t_coef = std::pow(e->prm.diffusion_length_mm / e->mesh.mean_edge, 2.0);
+    e->t = e->t_coef * e->mesh.mean_edge * e->mesh.mean_edge;
+    if (fcw::build_symbolic(e->mesh, e->prm.leaf_size, e->prm.max_width, e->prm.relax, e->sym, err)) return fail(FCW_E_INVALID, err);
+    e->analyze_ms = now_ms() - t0;
+    const auto& S = e->sym;
+    const auto& m = e->mesh;
+    if (S.max_ns > fcw::kMaxWidth) return fail(FCW_E_INVALID, "supernode wider than the kernels support");
+    e->ground_new = (int32_t)(S.n - 1);
+
+    FCW_CUDA(cudaSetDevice(e->device));
+    FCW_CUDA(fcw::configure_kernels());
+    FCW_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    FCW_TRY(e->dalloc(&e->err_d, 1));
+    FCW_CUDA(cudaMemset(e->err_d, 0, sizeof(int)));
+
+    // structure
+    int32_t *sn_c0, *sn_m, *rows, *sn_parent, *col_sn, *level_nodes, *child_ptr, *child_list, *relind, *seg_sn,
+        *seg_pos;
+    int64_t *sn_rowptr, *sn_valptr, *sn_invptr, *sn_updptr, *seg_ptr, *a_dst;
+    FCW_TRY(e->upload(&sn_c0, S.sn_c0));
+    FCW_TRY(e->upload(&sn_m, S.sn_m));
+    FCW_TRY(e->upload(&sn_rowptr, S.sn_rowptr));
+    FCW_TRY(e->upload(&rows, S.rows));
+    FCW_TRY(e->upload(&sn_valptr, S.sn_valptr));
+    FCW_TRY(e->upload(&sn_invptr, S.sn_invptr));
+    FCW_TRY(e->upload(&sn_updptr, S.sn_updptr));
+    FCW_TRY(e->upload(&sn_parent, S.sn_parent));
+    FCW_TRY(e->upload(&col_sn, S.col_sn));
+    FCW_TRY(e->upload(&level_nodes, S.level_nodes));
+    FCW_TRY(e->upload(&child_ptr, S.child_ptr));
+    FCW_TRY(e->upload(&child_list, S.child_list));
+    FCW_TRY(e->upload(&relind, S.relind));
+    FCW_TRY(e->upload(&seg_ptr, S.seg_ptr));
+    FCW_TRY(e->upload(&seg_sn, S.seg_sn));
+    FCW_TRY(e->upload(&seg_pos, S.seg_pos));
+    FCW_TRY(e->upload(&a_dst, S.a_dst));
+    fcw::DevPlan& P = e->plan;
+    P.n = (int32_t)S.n;
+    P.nsuper = S.nsuper;
+    P.nlevels = S.nlevels;
+    P.sn_c0 = sn_c0; P.sn_m = sn_m; P.sn_rowptr = sn_rowptr; P.rows = rows; P.sn_valptr = sn_valptr;
+    P.sn_invptr = sn_invptr; P.sn_updptr = sn_updptr; P.sn_parent = sn_parent; P.col_sn = col_sn;
+    P.level_nodes = level_nodes; P.child_ptr = child_ptr; P.child_list = child_list; P.relind = relind;
+    P.seg_ptr = seg_ptr; P.seg_sn = seg_sn; P.seg_pos = seg_pos;
+    e->level_tiles.assign(S.nlevels, 1);
+    for (int32_t l = 0; l < S.nlevels; ++l) {
+        int64_t mx = 1;
+        for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+            const int32_t s = S.level_nodes[q];
+            const int64_t nr = S.sn_m[s] - (S.sn_c0[s + 1] - S.sn_c0[s]);
+            const int64_t nt = (nr + 31) / 32;
+            mx = std::max<int64_t>(mx, nt * (nt + 1) / 2);
+        }
+        e->level_tiles[l] = (int32_t)std::min<int64_t>(mx, 512);
+    }
+
+    // mesh arrays in elimination order
+    const int64_t n = S.n;
+    std::vector<double> coords(3 * n), varea(n);
+    for (int64_t j = 0; j < n; ++j) {
+        const int32_t o = S.perm[j];
+        for (int c = 0; c < 3; ++c) coords[3 * j + c] = m.V[3 * (int64_t)o + c];
+        varea[j] = m.vertex_area[o];
+    }
+    std::vector<int32_t> fv(3 * nf), bnd(m.boundary.size());
+    for (int64_t i = 0; i < 3 * nf; ++i) fv[i] = S.iperm[m.F[i]];
+    for (size_t i = 0; i < m.boundary.size(); ++i) bnd[i] = S.iperm[m.boundary[i]];
+    std::vector<float> coef(4 * nf);
+    for (int64_t f = 0; f < nf; ++f) {
+        const double* g = &m.gb[9 * f];
+        const double c11 = g[3] * g[3] + g[4] * g[4] + g[5] * g[5];
+        const double c12 = g[3] * g[6] + g[4] * g[7] + g[5] * g[8];
+        const double c22 = g[6] * g[6] + g[7] * g[7] + g[8] * g[8];
+        coef[4 * f] = (float)c11; coef[4 * f + 1] = (float)c12; coef[4 * f + 2] = (float)c22;
+        coef[4 * f + 3] = (float)m.grad_area[f];
+    }
+    std::vector<int32_t> inc_ptr(n + 1, 0), inc_face(3 * nf);
+    std::vector<int8_t> inc_corner(3 * nf);
+    for (int64_t i = 0; i < 3 * nf; ++i) inc_ptr[fv[i] + 1]++;
+    for (int64_t j = 0; j < n; ++j) inc_ptr[j + 1] += inc_ptr[j];
+    {
+        std::vector<int32_t> fill(inc_ptr.begin(), inc_ptr.end() - 1);
+        for (int64_t f = 0; f < nf; ++f)
+            for (int c = 0; c < 3; ++c) {
+                const int32_t v = fv[3 * f + c];
+                inc_face[fill[v]] = (int32_t)f;
+                inc_corner[fill[v]] = (int8_t)c;
+                fill[v]++;
+            }
+    }
+    int32_t *fv_d, *inc_ptr_d, *inc_face_d;
+    int8_t* inc_corner_d;
+    double *gb_d, *garea_d;
+    float* coef_d;
+    FCW_TRY(e->upload(&fv_d, fv));
+    FCW_TRY(e->upload(&gb_d, m.gb));
+    FCW_TRY(e->upload(&garea_d, m.grad_area));
+    FCW_TRY(e->upload(&coef_d, coef));
+    FCW_TRY(e->upload(&inc_ptr_d, inc_ptr));
+    FCW_TRY(e->upload(&inc_face_d, inc_face));
+    FCW_TRY(e->upload(&inc_corner_d, inc_corner));
+    e->fd.nv = (int32_t)n; e->fd.nf = (int32_t)nf; e->fd.fv = fv_d; e->fd.gb = gb_d; e->fd.garea = garea_d;
+    e->fd.coef = coef_d; e->fd.inc_ptr = inc_ptr_d; e->fd.inc_face = inc_face_d; e->fd.inc_corner = inc_corner_d;
+    FCW_TRY(e->upload(&e->coords_d, coords));
+    FCW_TRY(e->upload(&e->varea_d, varea));
+    FCW_TRY(e->upload(&e->boundary_d, bnd));
+    FCW_TRY(e->upload(&e->farea_d, m.lean_area));
+    FCW_TRY(e->upload(&e->g11_d, m.g11));
+    FCW_TRY(e->upload(&e->g12_d, m.g12));
+    FCW_TRY(e->upload(&e->g22_d, m.g22));
+    FCW_TRY(e->upload(&e->iperm_d, S.iperm));
+    FCW_TRY(e->upload(&e->perm_d, S.perm));
+
+    // numeric factorisations
+    t0 = now_ms();
+    double *upd, *aval_d;
+    FCW_TRY(e->dalloc(&upd, S.n_upd));
+    FCW_TRY(e->dalloc(&aval_d, S.nnz_lower_a));
+    FCW_TRY(e->dalloc(&e->val_h, S.nnz_factor));
+    FCW_TRY(e->dalloc(&e->inv_h, S.n_inv));
+    FCW_TRY(e->dalloc(&e->val_p, S.nnz_factor));
+    FCW_TRY(e->dalloc(&e->inv_p, S.n_inv));
+    auto run_factor = [&](Op op, double* val, double* inv, const char* what) -> int {
+        std::vector<double> av = operator_values(e, op);
+        FCW_CUDA(cudaMemcpyAsync(aval_d, av.data(), av.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+        FCW_CUDA(cudaMemsetAsync(val, 0, S.nnz_factor * sizeof(double), e->stream));
+        FCW_CUDA(cudaMemsetAsync(upd, 0, std::max<int64_t>(S.n_upd, 1) * sizeof(double), e->stream));
+        fcw::launch_scatter_a(S.nnz_lower_a, a_dst, aval_d, val, e->stream);
+        for (int32_t l = 0; l < S.nlevels; ++l) {
+            const int32_t l0 = S.level_ptr[l], cnt = S.level_ptr[l + 1] - l0;
+            fcw::launch_factor_front(e->plan, l0, cnt, val, inv, upd, e->err_d, e->stream);
+            fcw::launch_factor_update(e->plan, l0, cnt, e->level_tiles[l], val, upd, e->stream);
+        }
+        FCW_CUDA(cudaGetLastError());
+        return check_kernel_errors(e, what);
+    };
+    FCW_TRY(run_factor(Op::Heat, e->val_h, e->inv_h, "heat factorisation"));
+    FCW_TRY(run_factor(Op::Poisson, e->val_p, e->inv_p, "Poisson factorisation"));
+    if (e->prm.build_mixed) {
+        double *val_tmp, *inv_tmp;
+        FCW_TRY(e->dalloc(&val_tmp, S.nnz_factor));
+        FCW_TRY(e->dalloc(&inv_tmp, S.n_inv));
+        FCW_TRY(run_factor(Op::Grounded, val_tmp, inv_tmp, "grounded Poisson factorisation"));
+        FCW_TRY(e->dalloc(&e->val_g, S.nnz_factor));
+        FCW_TRY(e->dalloc(&e->inv_g, S.n_inv));
+        fcw::launch_to_float(S.nnz_factor, val_tmp, e->val_g, e->stream);
+        fcw::launch_to_float(S.n_inv, inv_tmp, e->inv_g, e->stream);
+        FCW_CUDA(cudaStreamSynchronize(e->stream));
+        e->release(val_tmp);
+        e->release(inv_tmp);
+        e->bytes -= (int64_t)(S.nnz_factor + S.n_inv) * 8;
+    }
+    FCW_CUDA(cudaStreamSynchronize(e->stream));
+    e->release(upd);
+    e->release(aval_d);
+    e->bytes -= (int64_t)(std::max<int64_t>(S.n_upd, 1) + std::max<int64_t>(S.nnz_lower_a, 1)) * 8;
+    e->factor_ms = now_ms() - t0;
+    return FCW_OK;
+}
+
+int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
+    Workspace& w = e->ws;
+    if (w.K >= K && w.out_stride >= stride) return FCW_OK;
+    const int32_t Kn = std::max(K, w.K);
+    const int32_t sn = std::max(stride, w.out_stride);
+    void* old[] = {w.Bh, w.Bp64, w.Bp32, w.dT64, w.dT32, w.src, w.reach, w.band, w.longf, w.out};
+    for (void* p : old)
+        if (p) e->release(p);
+    w = Workspace{};
+    const int64_t n = e->sym.n, nf = e->mesh.nf;
+    FCW_TRY(e->dalloc(&w.Bh, (size_t)n * Kn));
+    FCW_TRY(e->dalloc(&w.Bp64, (size_t)n * Kn));
+    FCW_TRY(e->dalloc(&w.Bp32, (size_t)n * Kn));
+    FCW_TRY(e->dalloc(&w.dT64, (size_t)n * Kn));
+    FCW_TRY(e->dalloc(&w.dT32, (size_t)n * Kn));
+    FCW_TRY(e->dalloc(&w.src, (size_t)Kn));
+    FCW_TRY(e->dalloc(&w.reach, (size_t)std::max<int64_t>(e->sym.nsuper, 1)));
+    FCW_TRY(e->dalloc(&w.band, (size_t)nf * Kn));
+    FCW_TRY(e->dalloc(&w.longf, (size_t)nf * Kn));
+    FCW_TRY(e->dalloc(&w.out, (size_t)sn * Kn));
+    w.K = Kn;
+    w.out_stride = sn;
+    return FCW_OK;
+}
+
+// Heat solve for the K sources in ws.src: u (elimination order, n x K) in ws.Bh.
+void heat_solve(fcw_engine* e, int32_t K, cudaStream_t st) {
+    const auto& S = e->sym;
+    Workspace& w = e->ws;
+    mark(e, st, FCW_STAGE_HEAT_FWD);
+    fcw::launch_reach(e->plan, w.src, K, w.reach, st);
+    for (int32_t l = 0; l < S.nlevels; ++l)
+        fcw::launch_fwd_level<double>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], e->val_h,
+                                      e->inv_h, w.Bh, K, w.src, w.reach, st);
+    mark(e, st, FCW_STAGE_HEAT_BWD);
+    e->launches += 2 + 2 * (int64_t)S.nlevels;
+    for (int32_t l = S.nlevels - 1; l >= 0; --l)
+        fcw::launch_bwd_level<double>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], e->val_h,
+                                      e->inv_h, w.Bh, K, w.reach, st);
+}
+
+template <typename T>
+void poisson_solve(fcw_engine* e, const T* val, const T* inv, T* B, int32_t K, cudaStream_t st) {
+    const auto& S = e->sym;
+    mark(e, st, FCW_STAGE_POISSON_FWD);
+    for (int32_t l = 0; l < S.nlevels; ++l)
+        fcw::launch_fwd_level<T>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], val, inv, B, K,
+                                 nullptr, nullptr, st);
+    mark(e, st, FCW_STAGE_POISSON_BWD);
+    e->launches += 2 * (int64_t)S.nlevels;
+    for (int32_t l = S.nlevels - 1; l >= 0; --l)
+        fcw::launch_bwd_level<T>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], val, inv, B, K,
+                                 nullptr, st);
+}
+
+// Distances for the K sources in ws.src, shifted, source-major in ws.dT64 / ws.dT32.
+void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st) {
+    Workspace& w = e->ws;
+    const int32_t n = (int32_t)e->sym.n;
+    heat_solve(e, K, st);
+    mark(e, st, FCW_STAGE_DIVERGENCE);
+    if (precision == FCW_PREC_MIXED) {
+        fcw::launch_divergence_mixed(e->fd, w.Bh, w.Bp32, K, e->ground_new, st);
+        poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, K, st);
+        mark(e, st, FCW_STAGE_SHIFT);
+        fcw::launch_shift_transpose<float, float>(n, K, w.Bp32, w.src, w.dT32, st);
+    } else {
+        fcw::launch_divergence_fp64(e->fd, w.Bh, w.Bp64, K, st);
+        poisson_solve<double>(e, e->val_p, e->inv_p, w.Bp64, K, st);
+        mark(e, st, FCW_STAGE_SHIFT);
+        fcw::launch_shift_transpose<double, double>(n, K, w.Bp64, w.src, w.dT64, st);
+    }
+    e->launches += 2;
+}
+
+int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, double eps, int32_t nsrc,
+                fcw::MetricArgs& a) {
+    if (nt < 1 || nt > fcw::kMaxTargets) return fail(FCW_E_INVALID, "n_targets must be in [1, 32]");
+    if (nb < 0 || nb > fcw::kMaxBetween) return fail(FCW_E_INVALID, "n_between must be in [0, 8]");
+    if (!targets) return fail(FCW_E_INVALID, "targets is NULL");
+    for (int32_t i = 0; i + 1 < nt; ++i)
+        if (!(targets[i] <= targets[i + 1])) return fail(FCW_E_INVALID, "targets must be sorted ascending");
+    a = fcw::MetricArgs{};
+    a.n = (int32_t)e->sym.n;
+    a.nf = (int32_t)e->mesh.nf;
+    a.nsrc = nsrc;
+    a.stride = fcw_metrics_stride(nt, nb);
+    a.n_targets = nt;
+    a.n_between = nb;
+    a.n_boundary = (int32_t)e->mesh.boundary.size();
+    a.coords = e->coords_d;
+    a.vertex_area = e->varea_d;
+    a.boundary = e->boundary_d;
+    a.fv = e->fd.fv;
+    a.farea = e->farea_d;
+    a.g11 = e->g11_d;
+    a.g12 = e->g12_d;
+    a.g22 = e->g22_d;
+    a.width = e->mesh.bin_width;
+    a.health_h = e->mesh.health_h;
+    a.eps = eps;
+    a.rtol = 1e-10;
+    a.max_iter = 60;
+    for (int32_t i = 0; i < nt; ++i) a.targets[i] = targets[i];
+    for (int32_t j = 0; j < nb; ++j) a.fracs[j] = (double)(j + 1) / ((double)nb + 1.0);
+    a.src = e->ws.src;
+    a.band = e->ws.band;
+    a.longf = e->ws.longf;
+    a.out = e->ws.out;
+    a.err = e->err_d;
+    return FCW_OK;
+}
+
+template <typename T>
+void metrics_block(fcw_engine* e, fcw::MetricArgs& a, const T* dT, cudaStream_t st) {
+    mark(e, st, FCW_STAGE_VERTEX_STATS);
+    fcw::launch_vertex_stats<T>(a, dT, st);
+    mark(e, st, FCW_STAGE_GEOMETRY);
+    fcw::launch_geometry<T>(a, dT, st);
+    mark(e, st, -1);
+    e->launches += 2;
+}
+
+int check_engine(fcw_engine* e) {
+    if (!e) return fail(FCW_E_INVALID, "engine is NULL");
+    cudaError_t ce = cudaSetDevice(e->device);
+    if (ce != cudaSuccess) return fail(FCW_E_CUDA, cudaGetErrorString(ce));
+    return FCW_OK;
+}
+
+int map_sources_host(fcw_engine* e, const int32_t* sources, int64_t n, int32_t K, cudaStream_t st,
+                     std::vector<int32_t>& buf) {
+    buf.assign(K, -1);
+    for (int64_t k = 0; k < n; ++k) {
+        const int32_t s = sources[k];
+        if (s < 0 || s >= e->sym.n)
+            return fail(FCW_E_INVALID, "source_idx out of range: " + std::to_string(s) + " for mesh with " +
+                                           std::to_string(e->sym.n) + " vertices");
+        buf[k] = e->sym.iperm[s];
+    }
+    FCW_CUDA(cudaMemcpyAsync(e->ws.src, buf.data(), K * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    return FCW_OK;
+}
+
+int32_t round_k(int64_t k) { return (int32_t)(((k + 31) / 32) * 32); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void fcw_default_params(fcw_params* p) {
+    if (!p) return;
+    p->diffusion_length_mm = 0.7;
+    p->poisson_shift = 1e-10;
+    p->block_k = 256;
+    p->leaf_size = 64;
+    p->max_width = 64;
+    p->relax = 32;
+    p->build_mixed = 1;
+    p->device = 0;
+    p->refine_steps = 0;
+}
+
+int fcw_metrics_stride(int32_t n_targets, int32_t n_between) {
+    if (n_targets < 0 || n_between < 0) return 0;
+    const int32_t ne = n_targets > 0 ? (n_targets - 1) * n_between : 0;
+    return FCW_M_RADII + 2 * n_targets + 2 * ne;
+}
+
+int fcw_last_error(char* buf, size_t len) {
+    if (buf && len) {
+        std::strncpy(buf, g_err.c_str(), len - 1);
+        buf[len - 1] = '\0';
+    }
+    return (int)g_err.size();
+}
+
+int fcw_mesh_arrays(const double* V, int64_t nv, const int32_t* F, int64_t nf, double* vertex_area,
+                    double* lean_area, double* g11, double* g12, double* g22, uint8_t* boundary_flag) {
+    if (!V || !F) return fail(FCW_E_INVALID, "vertices/faces is NULL");
+    fcw::MeshPrep m;
+    std::string err;
+    if (fcw::prepare_mesh(V, nv, F, nf, m, err)) return fail(FCW_E_INVALID, err);
+    if (vertex_area) std::memcpy(vertex_area, m.vertex_area.data(), nv * sizeof(double));
+    if (lean_area) std::memcpy(lean_area, m.lean_area.data(), nf * sizeof(double));
+    if (g11) std::memcpy(g11, m.g11.data(), nf * sizeof(double));
+    if (g12) std::memcpy(g12, m.g12.data(), nf * sizeof(double));
+    if (g22) std::memcpy(g22, m.g22.data(), nf * sizeof(double));
+    if (boundary_flag) {
+        std::memset(boundary_flag, 0, nv);
+        for (int32_t b : m.boundary) boundary_flag[b] = 1;
+    }
+    return FCW_OK;
+}
+
+int fcw_analyze(const double* V, int64_t nv, const int32_t* F, int64_t nf, const fcw_params* params,
+                fcw_info* info, int32_t* perm_out) {
+    if (!V || !F) return fail(FCW_E_INVALID, "vertices/faces is NULL");
+    FCW_TRY(validate_params(params));
+    fcw::MeshPrep m;
+    fcw::Symbolic S;
+    std::string err;
+    double t0 = now_ms();
+    if (fcw::prepare_mesh(V, nv, F, nf, m, err)) return fail(FCW_E_INVALID, err);
+    if (fcw::build_symbolic(m, params->leaf_size, params->max_width, params->relax, S, err)) return fail(FCW_E_INVALID, err);
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->n_vertices = nv;
+        info->n_faces = nf;
+        info->n_boundary = (int64_t)m.boundary.size();
+        info->n_supernodes = S.nsuper;
+        info->n_levels = S.nlevels;
+        info->nnz_factor = S.nnz_factor;
+        info->nnz_l = S.nnz_l;
+        info->max_ns = S.max_ns;
+        info->max_m = S.max_m;
+        info->mean_edge_length = m.mean_edge;
+        info->t_coef = std::pow(params->diffusion_length_mm / m.mean_edge, 2.0);
+        info->t = info->t_coef * m.mean_edge * m.mean_edge;
+        info->bin_width = m.bin_width;
+        info->health_h = m.health_h;
+        info->total_vertex_area = m.total_area;
+        info->analyze_ms = now_ms() - t0;
+        info->flops_factor = S.flops_factor;
+    }
+    if (perm_out) std::memcpy(perm_out, S.perm.data(), nv * sizeof(int32_t));
+    return FCW_OK;
+}
+
+int fcw_engine_create(const double* V, int64_t nv, const int32_t* F, int64_t nf, const fcw_params* params,
+                      fcw_engine** out) {
+    if (!out) return fail(FCW_E_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!V || !F) return fail(FCW_E_INVALID, "vertices/faces is NULL");
+    FCW_TRY(validate_params(params));
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return fail(FCW_E_NODEVICE, std::string("no CUDA device available: ") + cudaGetErrorString(ce));
+    }
+    if (params->device < 0 || params->device >= ndev) return fail(FCW_E_INVALID, "invalid device ordinal");
+    fcw_engine* e = new fcw_engine();
+    e->prm = *params;
+    e->device = params->device;
+    int rc = build_engine(e, V, nv, F, nf);
+    if (rc == FCW_OK) rc = ensure_workspace(e, params->block_k, fcw_metrics_stride(12, 3));
+    if (rc != FCW_OK) {
+        std::string msg = g_err;
+        delete e;
+        g_err = msg;
+        return rc;
+    }
+    *out = e;
+    return FCW_OK;
+}
+
+int fcw_engine_info(const fcw_engine* e, fcw_info* info) {
+    if (!e || !info) return fail(FCW_E_INVALID, "NULL argument");
+    std::memset(info, 0, sizeof(*info));
+    const auto& S = e->sym;
+    const auto& m = e->mesh;
+    info->n_vertices = m.nv;
+    info->n_faces = m.nf;
+    info->n_boundary = (int64_t)m.boundary.size();
+    info->n_supernodes = S.nsuper;
+    info->n_levels = S.nlevels;
+    info->nnz_factor = S.nnz_factor;
+    info->nnz_l = S.nnz_l;
+    info->max_ns = S.max_ns;
+    info->max_m = S.max_m;
+    info->mean_edge_length = m.mean_edge;
+    info->t_coef = e->t_coef;
+    info->t = e->t;
+    info->bin_width = m.bin_width;
+    info->health_h = m.health_h;
+    info->total_vertex_area = m.total_area;
+    info->analyze_ms = e->analyze_ms;
+    info->factor_ms = e->factor_ms;
+    info->flops_factor = S.flops_factor;
+    info->device_bytes = e->bytes;
+    return FCW_OK;
+}
+
+int fcw_engine_destroy(fcw_engine* e) {
+    if (!e) return FCW_OK;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    delete e;
+    return FCW_OK;
+}
+
+int fcw_compute_distances(fcw_engine* e, const int32_t* sources, int64_t n, int32_t precision, double* out_host) {
+    FCW_TRY(check_engine(e));
+    if (n < 0 || (n > 0 && (!sources || !out_host))) return fail(FCW_E_INVALID, "NULL argument");
+    if (precision == FCW_PREC_MIXED && !e->val_g) return fail(FCW_E_INVALID, "engine was built without the mixed form");
+    const int32_t Kmax = e->prm.block_k;
+    const int64_t nv = e->sym.n;
+    std::vector<int32_t> buf;
+    std::vector<double> rowbuf(nv);
+    std::vector<float> rowbuf32(nv);
+    for (int64_t b0 = 0; b0 < n; b0 += Kmax) {
+        const int64_t nb = std::min<int64_t>(Kmax, n - b0);
+        const int32_t K = round_k(nb);
+        FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
+        FCW_TRY(map_sources_host(e, sources + b0, nb, K, e->stream, buf));
+        distances_block(e, K, precision, e->stream);
+        FCW_CUDA(cudaGetLastError());
+        for (int64_t r = 0; r < nb; ++r) {
+            if (precision == FCW_PREC_MIXED) {
+                FCW_CUDA(cudaMemcpyAsync(rowbuf32.data(), e->ws.dT32 + r * nv, nv * sizeof(float),
+                                         cudaMemcpyDeviceToHost, e->stream));
+                FCW_CUDA(cudaStreamSynchronize(e->stream));
+                for (int64_t i = 0; i < nv; ++i) out_host[(b0 + r) * nv + i] = (double)rowbuf32[e->sym.iperm[i]];
+            } else {
+                FCW_CUDA(cudaMemcpyAsync(rowbuf.data(), e->ws.dT64 + r * nv, nv * sizeof(double),
+                                         cudaMemcpyDeviceToHost, e->stream));
+                FCW_CUDA(cudaStreamSynchronize(e->stream));
+                for (int64_t i = 0; i < nv; ++i) out_host[(b0 + r) * nv + i] = rowbuf[e->sym.iperm[i]];
+            }
+        }
+        FCW_TRY(check_kernel_errors(e, "distances"));
+    }
+    return FCW_OK;
+}
+
+int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host) {
+    return fcw_compute_distances(e, &source, 1, FCW_PREC_FP64, out_host);
+}
+
+int fcw_compute_metrics(fcw_engine* e, const int32_t* sources, int64_t n, int32_t precision, const double* targets,
+                        int32_t nt, int32_t nb, double eps, double* out_host) {
+    FCW_TRY(check_engine(e));
+    if (n < 0 || (n > 0 && (!sources || !out_host))) return fail(FCW_E_INVALID, "NULL argument");
+    if (precision == FCW_PREC_MIXED && !e->val_g) return fail(FCW_E_INVALID, "engine was built without the mixed form");
+    const int32_t stride = fcw_metrics_stride(nt, nb);
+    const int32_t Kmax = e->prm.block_k;
+    std::vector<int32_t> buf;
+    for (int64_t b0 = 0; b0 < n; b0 += Kmax) {
+        const int64_t nbk = std::min<int64_t>(Kmax, n - b0);
+        const int32_t K = round_k(nbk);
+        FCW_TRY(ensure_workspace(e, K, stride));
+        fcw::MetricArgs a;
+        FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
+        FCW_TRY(map_sources_host(e, sources + b0, nbk, K, e->stream, buf));
+        distances_block(e, K, precision, e->stream);
+        if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, e->ws.dT32, e->stream);
+        else metrics_block<double>(e, a, e->ws.dT64, e->stream);
+        FCW_CUDA(cudaGetLastError());
+        FCW_CUDA(cudaMemcpyAsync(out_host + b0 * stride, e->ws.out, nbk * stride * sizeof(double),
+                                 cudaMemcpyDeviceToHost, e->stream));
+        FCW_TRY(check_kernel_errors(e, "metrics"));
+    }
+    return FCW_OK;
+}
+
+int fcw_compute_metrics_device(fcw_engine* e, const int32_t* sources_dev, int64_t n, int32_t precision,
+                               const double* targets, int32_t nt, int32_t nb, double eps, double* out_dev,
+                               void* stream) {
+    FCW_TRY(check_engine(e));
+    if (n < 0 || (n > 0 && (!sources_dev || !out_dev))) return fail(FCW_E_INVALID, "NULL argument");
+    if (precision == FCW_PREC_MIXED && !e->val_g) return fail(FCW_E_INVALID, "engine was built without the mixed form");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int32_t stride = fcw_metrics_stride(nt, nb);
+    const int32_t Kmax = e->prm.block_k;
+    for (int64_t b0 = 0; b0 < n; b0 += Kmax) {
+        const int64_t nbk = std::min<int64_t>(Kmax, n - b0);
+        const int32_t K = round_k(nbk);
+        FCW_TRY(ensure_workspace(e, K, stride));
+        fcw::MetricArgs a;
+        FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
+        a.out = out_dev + b0 * stride;
+        k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(nbk, sources_dev + b0, e->iperm_d, (int32_t)e->sym.n, K,
+                                                       e->ws.src, e->err_d);
+        e->launches += 1;
+        distances_block(e, K, precision, st);
+        if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, e->ws.dT32, st);
+        else metrics_block<double>(e, a, e->ws.dT64, st);
+        FCW_CUDA(cudaGetLastError());
+    }
+    return FCW_OK;
+}
+
+int fcw_engine_profile(fcw_engine* e, int enable) {
+    FCW_TRY(check_engine(e));
+    FCW_TRY(collect_marks(e));
+    e->prof_on = enable != 0;
+    for (double& x : e->stage_ms) x = 0.0;
+    e->launches = 0;
+    return FCW_OK;
+}
+
+int fcw_engine_stage_times(fcw_engine* e, double* ms_out, int32_t n, int64_t* launches) {
+    FCW_TRY(check_engine(e));
+    FCW_TRY(collect_marks(e));
+    for (int32_t i = 0; i < n && i < FCW_N_STAGES; ++i) ms_out[i] = e->stage_ms[i];
+    if (launches) *launches = e->launches;
+    return FCW_OK;
+}
+
+int fcw_synchronize(fcw_engine* e, void* stream) {
+    FCW_TRY(check_engine(e));
+    FCW_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    return check_kernel_errors(e, "device call");
+}
+
+int fcw_heat_solve_device(fcw_engine* e, const int32_t* sources_dev, int32_t k, double* u_dev, void* stream) {
+    FCW_TRY(check_engine(e));
+    if (k <= 0 || !sources_dev || !u_dev) return fail(FCW_E_INVALID, "invalid arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int32_t K = round_k(k);
+    FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
+    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->ws.src,
+                                                   e->err_d);
+    heat_solve(e, K, st);
+    // u_dev[old][c] = Bh[iperm[old]][c]
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, e->ws.Bh, K, e->iperm_d, u_dev, k, nullptr, st);
+    FCW_CUDA(cudaGetLastError());
+    return FCW_OK;
+}
+
+int fcw_divergence_device(fcw_engine* e, const double* u_dev, int32_t k, double* div_dev, void* stream) {
+    FCW_TRY(check_engine(e));
+    if (k <= 0 || !u_dev || !div_dev) return fail(FCW_E_INVALID, "invalid arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int32_t K = round_k(k);
+    FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
+    FCW_CUDA(cudaMemsetAsync(e->ws.Bh, 0, (size_t)e->sym.n * K * sizeof(double), st));
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, u_dev, k, nullptr, e->ws.Bh, K, e->iperm_d, st);
+    fcw::launch_divergence_fp64(e->fd, e->ws.Bh, e->ws.Bp64, K, st);
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, e->ws.Bp64, K, e->iperm_d, div_dev, k, nullptr, st);
+    FCW_CUDA(cudaGetLastError());
+    return FCW_OK;
+}
+
+int fcw_poisson_solve_device(fcw_engine* e, const double* div_dev, const int32_t* sources_dev, int32_t k,
+                             double* phi_dev, void* stream) {
+    FCW_TRY(check_engine(e));
+    if (k <= 0 || !div_dev || !sources_dev || !phi_dev) return fail(FCW_E_INVALID, "invalid arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int32_t K = round_k(k);
+    FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
+    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->ws.src,
+                                                   e->err_d);
+    FCW_CUDA(cudaMemsetAsync(e->ws.Bp64, 0, (size_t)e->sym.n * K * sizeof(double), st));
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, div_dev, k, nullptr, e->ws.Bp64, K, e->iperm_d, st);
+    poisson_solve<double>(e, e->val_p, e->inv_p, e->ws.Bp64, K, st);
+    fcw::launch_shift_transpose<double, double>((int32_t)e->sym.n, K, e->ws.Bp64, e->ws.src, e->ws.dT64, st);
+    // phi_dev[old][c] = dT[c][iperm[old]]: transpose back through the permute kernel, column by column
+    for (int32_t c = 0; c < k; ++c)
+        fcw::launch_permute_rows((int32_t)e->sym.n, 1, e->ws.dT64 + (int64_t)c * e->sym.n, 1, e->iperm_d,
+                                 phi_dev + c, k, nullptr, st);
+    FCW_CUDA(cudaGetLastError());
+    return FCW_OK;
+}
+
+int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* sources_dev, int32_t k,
+                             const double* targets, int32_t nt, int32_t nb, double eps, double* out_dev,
+                             void* stream) {
+    FCW_TRY(check_engine(e));
+    if (k <= 0 || !d_dev || !sources_dev || !out_dev) return fail(FCW_E_INVALID, "invalid arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int32_t K = round_k(k);
+    const int32_t stride = fcw_metrics_stride(nt, nb);
+    FCW_TRY(ensure_workspace(e, K, stride));
+    fcw::MetricArgs a;
+    FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
+    a.out = out_dev;
+    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->ws.src,
+                                                   e->err_d);
+    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)e->sym.n, k, K, d_dev, e->iperm_d, e->ws.dT64);
+    metrics_block<double>(e, a, e->ws.dT64, st);
+    FCW_CUDA(cudaGetLastError());
+    return FCW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+// Fused gradient -> normalise -> divergence over faces (fastcw_lean.py:416-442).
+//
+// Vertex-centric gather: warp = one vertex, lane = one right-hand side. Each
+// vertex walks its incident faces in ascending face order and recomputes the
+// face's unit gradient, so every output element is written exactly once, by
+// one thread, with the per-vertex summation order of the reference's face loop
+// (no atomics, deterministic).
+//
+// FP64 form: the reference's 3-vector arithmetic, operation for operation,
+// with explicit round-to-nearest intrinsics so the compiler cannot contract
+// into FMAs: given the same u, the divergence is bit-identical.
+//
+// Mixed form: X = -grad u / |grad u| is invariant to scaling u's differences,
+// so the two FP64 differences are rescaled by a power of two to O(1) (exact)
+// and the rest runs in FP32 in the intrinsic form:
+//   |g|^2 = du1^2 c11 + 2 du1 du2 c12 + du2^2 c22,  g . gb_c = du1 c1c + du2 c2c
+// with c_ab = gb_a . gb_b. This keeps the direction accurate where u is far
+// below FP32's range (u spans ~1e-130..1 on these meshes).
+#include "kernels.cuh"
+
+namespace fcw {
+
+namespace {
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+__global__ void __launch_bounds__(256) k_div_fp64(FaceData fd, const double* __restrict__ u,
+                                                  double* __restrict__ div, int32_t K) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int v = blockIdx.x * 8 + warp;
+    if (v >= fd.nv) return;
+    const int col = blockIdx.y * kSlice + lane;
+    double acc = 0.0;
+    for (int q = fd.inc_ptr[v]; q < fd.inc_ptr[v + 1]; ++q) {
+        const int f = fd.inc_face[q];
+        const int c = fd.inc_corner[q];
+        const int i0 = fd.fv[3 * f], i1 = fd.fv[3 * f + 1], i2 = fd.fv[3 * f + 2];
+        const double* g = fd.gb + 9 * (int64_t)f;
+        const double u0 = u[(int64_t)i0 * K + col];
+        const double du1 = sub(u[(int64_t)i1 * K + col], u0);
+        const double du2 = sub(u[(int64_t)i2 * K + col], u0);
+        const double gx = add(mul(du1, g[3]), mul(du2, g[6]));
+        const double gy = add(mul(du1, g[4]), mul(du2, g[7]));
+        const double gz = add(mul(du1, g[5]), mul(du2, g[8]));
+        const double nn = __dsqrt_rn(add(add(mul(gx, gx), mul(gy, gy)), mul(gz, gz)));
+        if (!(nn > 1e-300)) continue;
+        const double s = __ddiv_rn(-fd.garea[f], nn);
+        const double* b = g + 3 * c;
+        acc = add(acc, mul(s, add(add(mul(gx, b[0]), mul(gy, b[1])), mul(gz, b[2]))));
+    }
+    div[(int64_t)v * K + col] = acc;
+}
+
+// 2^-e for the binary exponent e of |x| (x normal, nonzero): exact scaling to [1, 2).
+__device__ __forceinline__ double unit_scale(double m) {
+    const long long bits = __double_as_longlong(m);
+    const int e = (int)((bits >> 52) & 0x7ff) - 1023;
+    return __longlong_as_double((long long)(1023 - e) << 52);
+}
+
+__global__ void __launch_bounds__(256) k_div_mixed(FaceData fd, const double* __restrict__ u,
+                                                   float* __restrict__ div, int32_t K, int32_t ground) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int v = blockIdx.x * 8 + warp;
+    if (v >= fd.nv) return;
+    const int col = blockIdx.y * kSlice + lane;
+    float acc = 0.0f;
+    if (v != ground) {
+        for (int q = fd.inc_ptr[v]; q < fd.inc_ptr[v + 1]; ++q) {
+            const int f = fd.inc_face[q];
+            const int c = fd.inc_corner[q];
+            const int i0 = fd.fv[3 * f], i1 = fd.fv[3 * f + 1], i2 = fd.fv[3 * f + 2];
+            const double u0 = u[(int64_t)i0 * K + col];
+            const double d1 = u[(int64_t)i1 * K + col] - u0;
+            const double d2 = u[(int64_t)i2 * K + col] - u0;
+            const double mx = fmax(fabs(d1), fabs(d2));
+            if (!(mx >= 2.2250738585072014e-308)) continue;  // zero (or subnormal) gradient
+            const double sc = unit_scale(mx);
+            const float a1 = (float)(d1 * sc), a2 = (float)(d2 * sc);
+            const float4 cf = reinterpret_cast<const float4*>(fd.coef)[f];  // c11, c12, c22, area
+            const float qn = a1 * a1 * cf.x + 2.0f * a1 * a2 * cf.y + a2 * a2 * cf.z;
+            if (!(qn > 0.0f)) continue;
+            float w1, w2;
+            if (c == 0) { w1 = -(cf.x + cf.y); w2 = -(cf.y + cf.z); }
+            else if (c == 1) { w1 = cf.x; w2 = cf.y; }
+            else { w1 = cf.y; w2 = cf.z; }
+            acc -= cf.w * (a1 * w1 + a2 * w2) * rsqrtf(qn);
+        }
+    }
+    div[(int64_t)v * K + col] = acc;
+}
+
+}  // namespace
+
+void launch_divergence_fp64(const FaceData& fd, const double* u, double* div, int32_t K, cudaStream_t st) {
+    if (fd.nv <= 0 || K <= 0) return;
+    k_div_fp64<<<dim3((fd.nv + 7) / 8, K / kSlice), 256, 0, st>>>(fd, u, div, K);
+}
+
+void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,
+                             cudaStream_t st) {
+    if (fd.nv <= 0 || K <= 0) return;
+    k_div_mixed<<<dim3((fd.nv + 7) / 8, K / kSlice), 256, 0, st>>>(fd, u, div, K, ground);
+}
+
+}  // namespace fcw

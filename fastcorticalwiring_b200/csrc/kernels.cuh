@@ -1,0 +1,117 @@
+// Device kernels of the heat-method pipeline and their host launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fcw {
+
+// Error bits a kernel may raise (OR-ed into a device word read by the host).
+enum : int {
+    KERR_NOT_SPD = 1,         // non-positive pivot in the numeric factorisation
+    KERR_HIST_OVERFLOW = 2,   // more distance bins than the geometry kernel holds
+    KERR_SCRATCH = 4,         // per-source face list overflow
+    KERR_ARGS = 8,            // inconsistent launch arguments
+};
+
+constexpr int kMaxWidth = 64;      // widest supernode the dense kernels accept
+constexpr int kSlice = 32;         // right-hand sides per CTA column slice (one per lane)
+constexpr int kMaxBins = 2048;     // distance bins per source held in shared memory
+constexpr int kMaxTargets = 32;
+constexpr int kMaxBetween = 8;
+
+// Supernodal structure on the device (all pointers device memory).
+struct DevPlan {
+    int32_t n = 0, nsuper = 0, nlevels = 0;
+    const int32_t* sn_c0 = nullptr;
+    const int32_t* sn_m = nullptr;
+    const int64_t* sn_rowptr = nullptr;
+    const int32_t* rows = nullptr;
+    const int64_t* sn_valptr = nullptr;
+    const int64_t* sn_invptr = nullptr;
+    const int64_t* sn_updptr = nullptr;
+    const int32_t* sn_parent = nullptr;
+    const int32_t* col_sn = nullptr;
+    const int32_t* level_nodes = nullptr;
+    const int32_t* child_ptr = nullptr;
+    const int32_t* child_list = nullptr;
+    const int32_t* relind = nullptr;
+    const int64_t* seg_ptr = nullptr;
+    const int32_t* seg_sn = nullptr;
+    const int32_t* seg_pos = nullptr;
+};
+
+// ---- numeric factorisation (factor.cu) ----
+// Per-device kernel attributes (large dynamic shared memory); call once per device.
+cudaError_t configure_kernels();
+void launch_scatter_a(int64_t nnz, const int64_t* dst, const double* aval, double* val, cudaStream_t st);
+// one level: extend-add children, dense Cholesky of the diagonal block, its inverse, L21
+void launch_factor_front(const DevPlan& p, int32_t l0, int32_t count, double* val, double* inv, double* upd,
+                         int* err, cudaStream_t st);
+// one level: update matrices U -= L21 L21^T
+void launch_factor_update(const DevPlan& p, int32_t l0, int32_t count, int32_t max_tiles, const double* val,
+                          double* upd, cudaStream_t st);
+void launch_to_float(int64_t n, const double* src, float* dst, cudaStream_t st);
+
+// ---- multi-RHS supernodal triangular solves (solve.cu) ----
+// Forward sweep of one level: B <- L^{-1} B on the level's supernodes (pull form).
+// delta_src (nullable): K column sources in elimination order (-1 = empty column);
+// when given, B's right-hand side is the delta matrix and is not read.
+// reach (nullable): only supernodes with reach != 0 are solved; others count as zero.
+template <typename T>
+void launch_fwd_level(const DevPlan& p, int32_t l0, int32_t count, const T* val, const T* inv, T* B, int32_t K,
+                      const int32_t* delta_src, const uint8_t* reach, cudaStream_t st);
+// Backward sweep of one level: B <- L^{-T} B; reach as above (zero forward result when unset).
+template <typename T>
+void launch_bwd_level(const DevPlan& p, int32_t l0, int32_t count, const T* val, const T* inv, T* B, int32_t K,
+                      const uint8_t* reach, cudaStream_t st);
+void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st);
+
+// ---- fused gradient -> normalise -> divergence (face.cu) ----
+struct FaceData {
+    int32_t nv = 0, nf = 0;
+    const int32_t* fv = nullptr;        // nf*3, elimination-order vertex ids
+    const double* gb = nullptr;         // nf*9 hat-function gradients (fastcw_lean.py:375-391)
+    const double* garea = nullptr;      // nf
+    const float* coef = nullptr;        // nf*4: c11, c12, c22, area (FP32 intrinsic form)
+    const int32_t* inc_ptr = nullptr;   // nv+1, per elimination-order vertex
+    const int32_t* inc_face = nullptr;  // incident faces in ascending face order
+    const int8_t* inc_corner = nullptr; // which corner of the face the vertex is
+};
+void launch_divergence_fp64(const FaceData& fd, const double* u, double* div, int32_t K, cudaStream_t st);
+void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,
+                             cudaStream_t st);
+
+// ---- per-source kernels (metrics.cu) ----
+template <typename Tin, typename Tout>
+void launch_shift_transpose(int32_t n, int32_t K, const Tin* phi, const int32_t* src, Tout* dT, cudaStream_t st);
+// out[out_idx[i]][c] = in[in_idx[i]][c] for i < n, c < cols (null index = identity)
+void launch_permute_rows(int32_t n, int32_t cols, const double* in, int32_t in_ld, const int32_t* in_idx,
+                         double* out, int32_t out_ld, const int32_t* out_idx, cudaStream_t st);
+
+struct MetricArgs {
+    int32_t n = 0, nf = 0, nsrc = 0, stride = 0, n_targets = 0, n_between = 0, n_boundary = 0;
+    const double* coords = nullptr;     // n*3, elimination order
+    const double* vertex_area = nullptr;
+    const int32_t* boundary = nullptr;  // elimination-order ids
+    const int32_t* fv = nullptr;
+    const double* farea = nullptr;      // lean face area, g11, g12, g22 (lean_geometry.py:44-63)
+    const double* g11 = nullptr;
+    const double* g12 = nullptr;
+    const double* g22 = nullptr;
+    double width = 0.0, health_h = 0.0, eps = 1e-6, rtol = 1e-10;
+    int32_t max_iter = 60;
+    double targets[kMaxTargets];
+    double fracs[kMaxBetween];
+    const int32_t* src = nullptr;       // elimination-order source per column
+    int32_t* band = nullptr;            // nsrc * nf scratch
+    int32_t* longf = nullptr;           // nsrc * nf scratch
+    double* out = nullptr;              // nsrc * stride
+    int* err = nullptr;
+};
+template <typename T>
+void launch_vertex_stats(const MetricArgs& a, const T* dT, cudaStream_t st);
+template <typename T>
+void launch_geometry(const MetricArgs& a, const T* dT, cudaStream_t st);
+
+}  // namespace fcw

@@ -17,7 +17,9 @@ Factorisation: the reference uses CHOLMOD when scikit-sparse is installed and
 SciPy SuperLU otherwise (fastcw_lean.py:445-464, 490-497). Neither CHOLMOD nor
 the production potpourri3d solver is installed here; the oracle factors with
 SciPy SuperLU in symmetric mode with no pivoting (the same matrix, an LDL-like
-factor), which agrees with the reference's pivoting SuperLU to FP64 rounding.
+factor) after a coordinate nested-dissection reordering, which agrees with the
+reference's pivoting SuperLU to FP64 rounding and factors large meshes in
+seconds instead of minutes.
 """
 
 from __future__ import annotations
@@ -123,17 +125,68 @@ def normalized_divergence(u, F, area, g0, g1, g2):
     return out
 
 
-class _SymmetricFactor:
-    """Sparse LU in SuperLU's symmetric mode (diagonal pivots, MMD on A + A^T)."""
+def coordinate_dissection(V, A, leaf=128):
+    """Fill-reducing order by recursive coordinate bisection of the vertex graph.
 
-    def __init__(self, A):
+    Each part is split at the median of its widest coordinate; the vertices of
+    the first half that touch the second half form the separator, numbered
+    last. Only the factorisation's speed depends on this order, never its result.
+    """
+    A = sp.csr_matrix(A, copy=True)
+    A.data = np.ones_like(A.data)  # pattern only (the stiffness has negative off-diagonals)
+    n = A.shape[0]
+    order = np.empty(n, dtype=np.int64)
+    side = np.zeros(n, dtype=np.int8)
+    stack = [(np.arange(n), 0, n)]
+    while stack:
+        verts, lo, hi = stack.pop()
+        if verts.size <= leaf:
+            order[lo:hi] = verts
+            continue
+        X = V[verts]
+        ax = int(np.argmax(X.max(axis=0) - X.min(axis=0)))
+        cut = np.median(X[:, ax])
+        first = X[:, ax] < cut
+        if first.all() or not first.any():
+            order[lo:hi] = verts
+            continue
+        side[verts] = 2
+        side[verts[first]] = 0
+        side[verts[~first]] = 1
+        touches = (A[verts[first]] @ (side == 1).astype(np.float64)) > 0
+        sep = verts[first][touches]
+        a = verts[first][~touches]
+        b = verts[~first]
+        side[verts] = 0
+        order[hi - sep.size:hi] = sep
+        stack.append((a, lo, lo + a.size))
+        stack.append((b, lo + a.size, lo + a.size + b.size))
+    return order
+
+
+class _SymmetricFactor:
+    """Sparse LU in SuperLU's symmetric mode (diagonal pivots) on a dissection-ordered matrix."""
+
+    def __init__(self, A, order=None):
         from scipy.sparse.linalg import splu
 
-        self._lu = splu(sp.csc_matrix(A), permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.0,
-                        options=dict(SymmetricMode=True))
+        A = sp.csc_matrix(A)
+        if order is None:
+            self._p = None
+            self._lu = splu(A, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.0, options=dict(SymmetricMode=True))
+        else:
+            self._p = np.asarray(order)
+            Ap = A[self._p][:, self._p].tocsc()
+            self._lu = splu(Ap, permc_spec="NATURAL", diag_pivot_thresh=0.0, options=dict(SymmetricMode=True))
 
     def solve(self, B):
-        return self._lu.solve(np.asfortranarray(B))
+        B = np.asarray(B)
+        if self._p is None:
+            return self._lu.solve(np.asfortranarray(B))
+        x = self._lu.solve(np.asfortranarray(B[self._p]))
+        out = np.empty_like(x)
+        out[self._p] = x
+        return out
 
 
 class HeatOracle:
@@ -144,7 +197,7 @@ class HeatOracle:
     Poisson operator L + shift * M (fastcw_lean.py:500).
     """
 
-    def __init__(self, V, F, diffusion_length_mm=0.7, poisson_shift=1e-10, t_coef=None):
+    def __init__(self, V, F, diffusion_length_mm=0.7, poisson_shift=1e-10, t_coef=None, ordering="dissection"):
         V = np.ascontiguousarray(V, dtype=np.float64)
         F = np.ascontiguousarray(F, dtype=np.int32)
         L, mass, area, g0, g1, g2 = operators(V, F)
@@ -157,8 +210,9 @@ class HeatOracle:
         self.L, self.mass = L, mass
         self.heat_matrix = (M + self.t * L).tocsc()
         self.poisson_matrix = (L + poisson_shift * M).tocsc()
-        self._heat = _SymmetricFactor(self.heat_matrix)
-        self._poisson = _SymmetricFactor(self.poisson_matrix)
+        order = coordinate_dissection(V, L) if ordering == "dissection" else None
+        self._heat = _SymmetricFactor(self.heat_matrix, order)
+        self._poisson = _SymmetricFactor(self.poisson_matrix, order)
         self.F, self.area, self.g0, self.g1, self.g2 = F, area, g0, g1, g2
         self.n_vertices = V.shape[0]
 

@@ -145,7 +145,8 @@ def _geometry_kat(ca, lg, tk):
     w = lg.default_bin_width(Vs, Fs)
     bufs = (np.empty(nF), np.empty(nF, np.int32), np.empty(nF, np.int32))
     rng = np.random.default_rng(1)
-    fields = [an._compute_geodesic_distances_from_subvertex(int(s)) for s in rng.choice(len(Vs), 3, replace=False)]
+    field_sources = [int(s) for s in rng.choice(len(Vs), 3, replace=False)] + [7]
+    fields = [an._compute_geodesic_distances_from_subvertex(s) for s in field_sources[:3]]
     d = an._compute_geodesic_distances_from_subvertex(7).copy()
     bad = rng.choice(len(d), len(d) // 50, replace=False)
     d[bad] += rng.uniform(0, 15, bad.size)
@@ -179,7 +180,7 @@ def _geometry_kat(ca, lg, tk):
     r_big, _ = lg.solve_radius(pre[nb] * 2, f, Fs, area, w, nb, ptr, pre, bufs[1], bufs[0], bufs[2], nl, 1e-12, 60)
     r_zero, _ = lg.solve_radius(0.0, f, Fs, area, w, nb, ptr, pre, bufs[1], bufs[0], bufs[2], nl, 1e-12, 60)
     return dict(
-        V=Vs, F=Fs, fields=fields, radii_eval=radii, area_eval=np.array(A), darea_eval=np.array(DA),
+        V=Vs, F=Fs, fields=fields, field_sources=np.array(field_sources), radii_eval=radii, area_eval=np.array(A), darea_eval=np.array(DA),
         perim_eval=np.array(P), n_long=np.array(NL), bin_width=w, targets=T, fracs=fr,
         geo_radii=np.array([g[0] for g in G]), geo_perim=np.array([g[1] for g in G]),
         geo_extra_r=np.array([g[2] for g in G]), geo_extra_a=np.array([g[3] for g in G]),

@@ -1,0 +1,114 @@
+"""C-ABI surface and host-side logic, no GPU needed."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from fastcorticalwiring_b200 import _lib, engine, mesh as M
+from tests.conftest import GOLDEN, ROOT
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "fcw_b200.h")).read()
+    return set(re.findall(r"^\s*(?:int|void)\s+(fcw_\w+)\s*\(", text, flags=re.M))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = _lib.load()
+    declared = _declared_symbols()
+    assert declared == set(_lib.EXPORTED)
+    for name in declared:
+        assert getattr(lib, name) is not None
+
+
+def test_params_struct_matches_defaults():
+    p = _lib.default_params()
+    assert p.diffusion_length_mm == 0.7 and p.poisson_shift == 1e-10
+    assert p.block_k % 32 == 0 and 1 <= p.relax <= p.max_width <= 64
+    assert _lib.metrics_stride(12, 3) == 7 + 24 + 66
+
+
+def _l4():
+    z = np.load(os.path.join(GOLDEN, "golden_heat_L4.npz"))
+    return z, M.prepare(z["V"], z["F"], z["mask"])
+
+
+def test_native_mesh_arrays_match_reference_bit_exact():
+    z, pm = _l4()
+    arr = _lib.mesh_arrays(pm.V, pm.F)
+    assert np.array_equal(arr["vertex_area"], z["vertex_area"])
+    assert np.array_equal(arr["boundary"], z["boundary"])
+    assert np.array_equal(arr["lean_area"], pm.lean_area)
+    for g in ("g11", "g12", "g22"):
+        assert np.array_equal(arr[g], getattr(pm, g))
+
+
+def test_analysis_info_matches_reference_quantities():
+    z, pm = _l4()
+    info, perm = _lib.analyze(pm.V, pm.F)
+    assert info["bin_width"] == float(z["bin_width"])
+    assert info["health_h"] == float(z["health_h"])
+    assert abs(info["t"] - float(z["t"])) <= 1e-15
+    assert sorted(perm.tolist()) == list(range(pm.n_vertices))
+    assert info["max_ns"] <= 64
+
+
+def test_quantile_matches_numpy_on_random_meshes():
+    rng = np.random.default_rng(4)
+    for level in (2, 3):
+        from fastcorticalwiring_b200.meshgen import folded_icosphere
+        m = folded_icosphere(level, seed=int(rng.integers(100)), jitter=0.2)
+        pm = M.prepare(m.vertices, m.faces, m.cortex_mask)
+        info, _ = _lib.analyze(pm.V, pm.F)
+        assert info["bin_width"] == pm.bin_width
+        assert info["health_h"] == pm.health_h
+
+
+@pytest.mark.parametrize("level", [3, 4, 5])
+def test_symbolic_structure_contains_true_fill(level):
+    """Every nonzero of the exact Cholesky factor lies inside the supernodal structure."""
+    import scipy.sparse as sp
+    from scipy.sparse.linalg import splu
+    import oracle
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+    m = folded_icosphere(level, seed=level, jitter=0.2)
+    pm = M.prepare(m.vertices, m.faces, m.cortex_mask)
+    info, perm = _lib.analyze(pm.V, pm.F)
+    L, mass, *_ = oracle.operators(pm.V, pm.F)
+    A = (sp.diags(mass) + 0.49 * L).tocsc()[perm][:, perm].tocsc()
+    lu = splu(A, permc_spec="NATURAL", diag_pivot_thresh=0.0, options=dict(SymmetricMode=True))
+    assert np.array_equal(lu.perm_c, np.arange(A.shape[0]))      # no reordering happened
+    assert lu.L.nnz <= info["nnz_l"]
+
+
+def test_engine_kwarg_rules_follow_potpourri_engine():
+    z, pm = _l4()
+    for bad in ({"use_robust": True}, {"t_coef": 1.0}, {"diffusion_length_mm": 0.4},
+                {"diffusion_length_mm": float("nan")}, {"not_a_setting": 1}):
+        with pytest.raises(ValueError):
+            engine.B200DistanceEngine(pm.V, pm.F, **bad)
+
+
+def test_unknown_engine_name_is_rejected():
+    with pytest.raises(ValueError, match="Unknown engine_type 'batch_heat'"):
+        engine.create_distance_engine("batch_heat", np.zeros((3, 3)), np.array([[0, 1, 2]]))
+    assert not hasattr(engine.BaseDistanceEngine, "compute_distance_batch")
+
+
+def test_no_cpu_fallback_without_a_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    z, pm = _l4()
+    with pytest.raises(_lib.FCWError) as ei:
+        engine.HeatEngine(pm.V, pm.F)
+    assert ei.value.code == _lib.FCW_E_NODEVICE
+
+
+def test_invalid_mesh_is_rejected_at_the_boundary():
+    V = np.zeros((3, 3))
+    with pytest.raises(_lib.FCWError) as ei:
+        _lib.analyze(V, np.array([[0, 1, 5]], dtype=np.int32))
+    assert ei.value.code == _lib.FCW_E_INVALID and "out of range" in str(ei.value)
