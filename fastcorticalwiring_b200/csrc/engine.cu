@@ -74,6 +74,7 @@ struct Workspace {
     double* Bh = nullptr;
     double* Bp64 = nullptr;
     float* Bp32 = nullptr;
+    double* Y = nullptr;        // Poisson solution (n x K doubles, or floats for the mixed form)
     double* dT64 = nullptr;
     float* dT32 = nullptr;
     int32_t* src = nullptr;
@@ -82,6 +83,9 @@ struct Workspace {
     int32_t* longf = nullptr;
     double* out = nullptr;
     int32_t out_stride = 0;
+    double* U = nullptr;        // forward update rows, (sum nr) x K doubles (reused as floats)
+    double* part = nullptr;     // backward split-K partial sums
+    int* counters = nullptr;    // split-K arrival tickets, zero at rest
 };
 
 struct fcw_engine {
@@ -96,6 +100,14 @@ struct fcw_engine {
     int64_t bytes = 0;
     fcw::DevPlan plan;
     std::vector<int32_t> level_tiles;
+    // solve schedule: per level, task ranges of the forward / backward task lists
+    std::vector<int32_t> fwd_ptr, bwd_ptr;
+    int2 *fwd_tasks = nullptr, *bwd_tasks = nullptr;
+    int64_t* uoff_d = nullptr;
+    int64_t* poff_d = nullptr;
+    int32_t* nsplit_d = nullptr;
+    int32_t *gm_ptr_d = nullptr, *gm_src_d = nullptr, *gm_child_d = nullptr;
+    int64_t n_urows = 0, n_parts = 0;
     double *val_h = nullptr, *inv_h = nullptr, *val_p = nullptr, *inv_p = nullptr;
     float *val_g = nullptr, *inv_g = nullptr;
     fcw::FaceData fd;
@@ -205,8 +217,8 @@ int validate_params(const fcw_params* p) {
     if (!std::isfinite(p->diffusion_length_mm) || p->diffusion_length_mm < 0.5)
         return fail(FCW_E_INVALID, "diffusion_length_mm must be finite and at least 0.5 mm.");
     if (!std::isfinite(p->poisson_shift) || p->poisson_shift < 0.0) return fail(FCW_E_INVALID, "invalid poisson_shift");
-    if (p->block_k < 32 || p->block_k % 32 != 0 || p->block_k > 4096)
-        return fail(FCW_E_INVALID, "block_k must be a multiple of 32 in [32, 4096]");
+    if (p->block_k < 64 || p->block_k % 64 != 0 || p->block_k > 4096)
+        return fail(FCW_E_INVALID, "block_k must be a multiple of 64 in [64, 4096]");
     if (p->leaf_size < 1 || p->max_width < 1 || p->max_width > fcw::kMaxWidth)
         return fail(FCW_E_INVALID, "max_width must be in [1, 64] and leaf_size >= 1");
     if (p->relax < 1 || p->relax > p->max_width) return fail(FCW_E_INVALID, "relax must be in [1, max_width]");
@@ -263,6 +275,7 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
 
     FCW_CUDA(cudaSetDevice(e->device));
     FCW_CUDA(fcw::configure_kernels());
+    FCW_CUDA(fcw::configure_solve_kernels());
     FCW_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     FCW_TRY(e->dalloc(&e->err_d, 1));
     FCW_CUDA(cudaMemset(e->err_d, 0, sizeof(int)));
@@ -306,6 +319,68 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
             mx = std::max<int64_t>(mx, nt * (nt + 1) / 2);
         }
         e->level_tiles[l] = (int32_t)std::min<int64_t>(mx, 512);
+    }
+
+    // solve schedule (see solve.cu): forward row-chunk tasks, backward split-K tasks,
+    // update-row offsets and the per-front-row gather lists of children's update rows
+    {
+        const int32_t NS = S.nsuper;
+        std::vector<int64_t> uoff(NS + 1, 0), poff(NS, 0);
+        std::vector<int32_t> nsplit(NS, 1);
+        int64_t parts = 0;
+        for (int32_t s = 0; s < NS; ++s) {
+            const int32_t ns = S.sn_c0[s + 1] - S.sn_c0[s], nr = S.sn_m[s] - ns;
+            uoff[s + 1] = uoff[s] + nr;
+            nsplit[s] = std::max(1, (nr + fcw::kSplitRows - 1) / fcw::kSplitRows);
+            poff[s] = parts;
+            if (nsplit[s] > 1) parts += nsplit[s];
+        }
+        e->n_urows = uoff[NS];
+        e->n_parts = parts;
+        std::vector<int2> ft, bt;
+        e->fwd_ptr.assign(S.nlevels + 1, 0);
+        e->bwd_ptr.assign(S.nlevels + 1, 0);
+        for (int32_t l = 0; l < S.nlevels; ++l) {
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+                const int32_t s = S.level_nodes[q];
+                const int32_t ns = S.sn_c0[s + 1] - S.sn_c0[s], nr = S.sn_m[s] - ns;
+                const int32_t nch = std::max(1, (nr + fcw::kMaxWidth - 1) / fcw::kMaxWidth);
+                for (int32_t c = 0; c < nch; ++c) ft.push_back(make_int2(s, c));
+                for (int32_t c = 0; c < nsplit[s]; ++c) bt.push_back(make_int2(s, c));
+            }
+            e->fwd_ptr[l + 1] = (int32_t)ft.size();
+            e->bwd_ptr[l + 1] = (int32_t)bt.size();
+        }
+        const int64_t nfront = S.sn_rowptr[NS];
+        std::vector<int32_t> gptr(nfront + 1, 0), gsrc(e->n_urows), gchild(e->n_urows);
+        for (int32_t c = 0; c < NS; ++c) {
+            const int32_t p = S.sn_parent[c];
+            const int32_t nsc = S.sn_c0[c + 1] - S.sn_c0[c];
+            for (int64_t q = S.sn_rowptr[c] + nsc; q < S.sn_rowptr[c + 1]; ++q) gptr[S.sn_rowptr[p] + S.relind[q] + 1]++;
+        }
+        for (int64_t g = 0; g < nfront; ++g) gptr[g + 1] += gptr[g];
+        {
+            std::vector<int32_t> fill(gptr.begin(), gptr.end() - 1);
+            for (int32_t c = 0; c < NS; ++c) {
+                const int32_t p = S.sn_parent[c];
+                const int32_t nsc = S.sn_c0[c + 1] - S.sn_c0[c];
+                for (int64_t q = S.sn_rowptr[c] + nsc; q < S.sn_rowptr[c + 1]; ++q) {
+                    const int64_t g = S.sn_rowptr[p] + S.relind[q];
+                    gsrc[fill[g]] = (int32_t)(uoff[c] + (q - S.sn_rowptr[c] - nsc));
+                    gchild[fill[g]] = c;
+                    fill[g]++;
+                }
+            }
+        }
+        if (e->n_urows > INT32_MAX || nfront > INT32_MAX) return fail(FCW_E_INVALID, "mesh too large for 32-bit update indices");
+        FCW_TRY(e->upload(&e->fwd_tasks, ft));
+        FCW_TRY(e->upload(&e->bwd_tasks, bt));
+        FCW_TRY(e->upload(&e->uoff_d, uoff));
+        FCW_TRY(e->upload(&e->poff_d, poff));
+        FCW_TRY(e->upload(&e->nsplit_d, nsplit));
+        FCW_TRY(e->upload(&e->gm_ptr_d, gptr));
+        FCW_TRY(e->upload(&e->gm_src_d, gsrc));
+        FCW_TRY(e->upload(&e->gm_child_d, gchild));
     }
 
     // mesh arrays in elimination order
@@ -417,7 +492,8 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
     if (w.K >= K && w.out_stride >= stride) return FCW_OK;
     const int32_t Kn = std::max(K, w.K);
     const int32_t sn = std::max(stride, w.out_stride);
-    void* old[] = {w.Bh, w.Bp64, w.Bp32, w.dT64, w.dT32, w.src, w.reach, w.band, w.longf, w.out};
+    void* old[] = {w.Bh, w.Bp64, w.Bp32, w.Y, w.dT64, w.dT32, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
+                   w.counters};
     for (void* p : old)
         if (p) e->release(p);
     w = Workspace{};
@@ -425,6 +501,7 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
     FCW_TRY(e->dalloc(&w.Bh, (size_t)n * Kn));
     FCW_TRY(e->dalloc(&w.Bp64, (size_t)n * Kn));
     FCW_TRY(e->dalloc(&w.Bp32, (size_t)n * Kn));
+    FCW_TRY(e->dalloc(&w.Y, (size_t)n * Kn));
     FCW_TRY(e->dalloc(&w.dT64, (size_t)n * Kn));
     FCW_TRY(e->dalloc(&w.dT32, (size_t)n * Kn));
     FCW_TRY(e->dalloc(&w.src, (size_t)Kn));
@@ -432,39 +509,72 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
     FCW_TRY(e->dalloc(&w.band, (size_t)nf * Kn));
     FCW_TRY(e->dalloc(&w.longf, (size_t)nf * Kn));
     FCW_TRY(e->dalloc(&w.out, (size_t)sn * Kn));
+    FCW_TRY(e->dalloc(&w.U, (size_t)std::max<int64_t>(e->n_urows, 1) * Kn));
+    FCW_TRY(e->dalloc(&w.part, (size_t)std::max<int64_t>(e->n_parts, 1) * fcw::kMaxWidth * Kn));
+    const int64_t nctr = (int64_t)std::max<int32_t>(e->sym.nsuper, 1) * (Kn / fcw::kRhsTile);
+    FCW_TRY(e->dalloc(&w.counters, (size_t)nctr));
+    FCW_CUDA(cudaMemset(w.counters, 0, nctr * sizeof(int)));
     w.K = Kn;
     w.out_stride = sn;
     return FCW_OK;
 }
 
-// Heat solve for the K sources in ws.src: u (elimination order, n x K) in ws.Bh.
-void heat_solve(fcw_engine* e, int32_t K, cudaStream_t st) {
-    const auto& S = e->sym;
-    Workspace& w = e->ws;
-    mark(e, st, FCW_STAGE_HEAT_FWD);
-    fcw::launch_reach(e->plan, w.src, K, w.reach, st);
-    for (int32_t l = 0; l < S.nlevels; ++l)
-        fcw::launch_fwd_level<double>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], e->val_h,
-                                      e->inv_h, w.Bh, K, w.src, w.reach, st);
-    mark(e, st, FCW_STAGE_HEAT_BWD);
-    e->launches += 2 + 2 * (int64_t)S.nlevels;
-    for (int32_t l = S.nlevels - 1; l >= 0; --l)
-        fcw::launch_bwd_level<double>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], e->val_h,
-                                      e->inv_h, w.Bh, K, w.reach, st);
+template <typename T>
+fcw::SolveArgs<T> solve_args(fcw_engine* e, const T* val, const T* inv, T* B, int32_t K) {
+    fcw::SolveArgs<T> a;
+    a.p = e->plan;
+    a.val = val;
+    a.inv = inv;
+    a.B = B;
+    a.K = K;
+    a.U = reinterpret_cast<T*>(e->ws.U);
+    a.uoff = e->uoff_d;
+    a.gm_ptr = e->gm_ptr_d;
+    a.gm_src = e->gm_src_d;
+    a.gm_child = e->gm_child_d;
+    a.nsplit = e->nsplit_d;
+    a.poff = e->poff_d;
+    a.part = reinterpret_cast<T*>(e->ws.part);
+    a.counters = e->ws.counters;
+    a.ktiles = e->ws.K / fcw::kRhsTile;
+    return a;
 }
 
 template <typename T>
-void poisson_solve(fcw_engine* e, const T* val, const T* inv, T* B, int32_t K, cudaStream_t st) {
+void sweep(fcw_engine* e, fcw::SolveArgs<T> a, cudaStream_t st, int stage_fwd, int stage_bwd) {
     const auto& S = e->sym;
-    mark(e, st, FCW_STAGE_POISSON_FWD);
-    for (int32_t l = 0; l < S.nlevels; ++l)
-        fcw::launch_fwd_level<T>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], val, inv, B, K,
-                                 nullptr, nullptr, st);
-    mark(e, st, FCW_STAGE_POISSON_BWD);
+    mark(e, st, stage_fwd);
+    for (int32_t l = 0; l < S.nlevels; ++l) {
+        a.tasks = e->fwd_tasks;
+        fcw::launch_fwd_level<T>(a, e->fwd_ptr[l], e->fwd_ptr[l + 1] - e->fwd_ptr[l], st);
+    }
+    a.delta_src = nullptr;
+    mark(e, st, stage_bwd);
+    for (int32_t l = S.nlevels - 1; l >= 0; --l) {
+        a.tasks = e->bwd_tasks;
+        fcw::launch_bwd_level<T>(a, e->bwd_ptr[l], e->bwd_ptr[l + 1] - e->bwd_ptr[l], st);
+    }
     e->launches += 2 * (int64_t)S.nlevels;
-    for (int32_t l = S.nlevels - 1; l >= 0; --l)
-        fcw::launch_bwd_level<T>(e->plan, S.level_ptr[l], S.level_ptr[l + 1] - S.level_ptr[l], val, inv, B, K,
-                                 nullptr, st);
+}
+
+// Heat solve for the K sources in ws.src: u (elimination order, n x K) in ws.Bh.
+void heat_solve(fcw_engine* e, int32_t K, cudaStream_t st) {
+    Workspace& w = e->ws;
+    mark(e, st, FCW_STAGE_HEAT_FWD);
+    fcw::launch_reach(e->plan, w.src, K, w.reach, st);
+    e->launches += 2;
+    fcw::SolveArgs<double> a = solve_args<double>(e, e->val_h, e->inv_h, w.Bh, K);
+    a.delta_src = w.src;
+    a.reach = w.reach;
+    sweep<double>(e, a, st, FCW_STAGE_HEAT_FWD, FCW_STAGE_HEAT_BWD);
+}
+
+// Poisson solve: right-hand sides R, solution into Y (both n x K, elimination order).
+template <typename T>
+void poisson_solve(fcw_engine* e, const T* val, const T* inv, const T* R, T* Y, int32_t K, cudaStream_t st) {
+    fcw::SolveArgs<T> a = solve_args<T>(e, val, inv, Y, K);
+    a.R = R;
+    sweep<T>(e, a, st, FCW_STAGE_POISSON_FWD, FCW_STAGE_POISSON_BWD);
 }
 
 // Distances for the K sources in ws.src, shifted, source-major in ws.dT64 / ws.dT32.
@@ -474,15 +584,16 @@ void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st) {
     heat_solve(e, K, st);
     mark(e, st, FCW_STAGE_DIVERGENCE);
     if (precision == FCW_PREC_MIXED) {
+        float* Y = reinterpret_cast<float*>(w.Y);
         fcw::launch_divergence_mixed(e->fd, w.Bh, w.Bp32, K, e->ground_new, st);
-        poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, K, st);
+        poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, Y, K, st);
         mark(e, st, FCW_STAGE_SHIFT);
-        fcw::launch_shift_transpose<float, float>(n, K, w.Bp32, w.src, w.dT32, st);
+        fcw::launch_shift_transpose<float, float>(n, K, Y, w.src, w.dT32, st);
     } else {
         fcw::launch_divergence_fp64(e->fd, w.Bh, w.Bp64, K, st);
-        poisson_solve<double>(e, e->val_p, e->inv_p, w.Bp64, K, st);
+        poisson_solve<double>(e, e->val_p, e->inv_p, w.Bp64, w.Y, K, st);
         mark(e, st, FCW_STAGE_SHIFT);
-        fcw::launch_shift_transpose<double, double>(n, K, w.Bp64, w.src, w.dT64, st);
+        fcw::launch_shift_transpose<double, double>(n, K, w.Y, w.src, w.dT64, st);
     }
     e->launches += 2;
 }
@@ -556,7 +667,7 @@ int map_sources_host(fcw_engine* e, const int32_t* sources, int64_t n, int32_t K
     return FCW_OK;
 }
 
-int32_t round_k(int64_t k) { return (int32_t)(((k + 31) / 32) * 32); }
+int32_t round_k(int64_t k) { return (int32_t)(((k + fcw::kRhsTile - 1) / fcw::kRhsTile) * fcw::kRhsTile); }
 
 }  // namespace
 
@@ -861,8 +972,8 @@ int fcw_poisson_solve_device(fcw_engine* e, const double* div_dev, const int32_t
                                                    e->err_d);
     FCW_CUDA(cudaMemsetAsync(e->ws.Bp64, 0, (size_t)e->sym.n * K * sizeof(double), st));
     fcw::launch_permute_rows((int32_t)e->sym.n, k, div_dev, k, nullptr, e->ws.Bp64, K, e->iperm_d, st);
-    poisson_solve<double>(e, e->val_p, e->inv_p, e->ws.Bp64, K, st);
-    fcw::launch_shift_transpose<double, double>((int32_t)e->sym.n, K, e->ws.Bp64, e->ws.src, e->ws.dT64, st);
+    poisson_solve<double>(e, e->val_p, e->inv_p, e->ws.Bp64, e->ws.Y, K, st);
+    fcw::launch_shift_transpose<double, double>((int32_t)e->sym.n, K, e->ws.Y, e->ws.src, e->ws.dT64, st);
     // phi_dev[old][c] = dT[c][iperm[old]]: transpose back through the permute kernel, column by column
     for (int32_t c = 0; c < k; ++c)
         fcw::launch_permute_rows((int32_t)e->sym.n, 1, e->ws.dT64 + (int64_t)c * e->sym.n, 1, e->iperm_d,

@@ -54,17 +54,39 @@ void launch_factor_update(const DevPlan& p, int32_t l0, int32_t count, int32_t m
 void launch_to_float(int64_t n, const double* src, float* dst, cudaStream_t st);
 
 // ---- multi-RHS supernodal triangular solves (solve.cu) ----
-// Forward sweep of one level: B <- L^{-1} B on the level's supernodes (pull form).
-// delta_src (nullable): K column sources in elimination order (-1 = empty column);
-// when given, B's right-hand side is the delta matrix and is not read.
-// reach (nullable): only supernodes with reach != 0 are solved; others count as zero.
+constexpr int kRhsTile = 64;     // right-hand sides per solve CTA; K is a multiple of this
+constexpr int kSplitRows = 128;  // structure rows per backward split-K task
+
 template <typename T>
-void launch_fwd_level(const DevPlan& p, int32_t l0, int32_t count, const T* val, const T* inv, T* B, int32_t K,
-                      const int32_t* delta_src, const uint8_t* reach, cudaStream_t st);
-// Backward sweep of one level: B <- L^{-T} B; reach as above (zero forward result when unset).
+struct SolveArgs {
+    DevPlan p;
+    const T* val = nullptr;          // panels
+    const T* inv = nullptr;          // inverse diagonal blocks
+    const T* R = nullptr;            // n x K right-hand sides (read only; unused with delta_src)
+    T* B = nullptr;                  // n x K forward result, then solution (elimination order)
+    int32_t K = 0;
+    T* U = nullptr;                  // forward update rows, (sum nr) x K
+    const int64_t* uoff = nullptr;   // first update row of each supernode
+    const int32_t* gm_ptr = nullptr; // per front row (sn_rowptr-based index): update rows that land on it
+    const int32_t* gm_src = nullptr;
+    const int32_t* gm_child = nullptr;
+    const int32_t* delta_src = nullptr;  // forward: identity columns for these sources (elimination order)
+    const uint8_t* reach = nullptr;      // supernodes on a source's path to the root (heat solve)
+    const int2* tasks = nullptr;         // (supernode, row chunk | split)
+    const int32_t* nsplit = nullptr;     // backward splits per supernode
+    const int64_t* poff = nullptr;       // partial-sum slot of the first split (units of 64 x K)
+    T* part = nullptr;
+    int* counters = nullptr;             // per (supernode, column tile) arrival tickets, zero at rest
+    int32_t ktiles = 0;                  // column tiles the counters were sized for
+};
+
+cudaError_t configure_solve_kernels();
+// Forward sweep of one level (tasks [t0, t0+ntasks) of the level's list).
 template <typename T>
-void launch_bwd_level(const DevPlan& p, int32_t l0, int32_t count, const T* val, const T* inv, T* B, int32_t K,
-                      const uint8_t* reach, cudaStream_t st);
+void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st);
+// Backward sweep of one level.
+template <typename T>
+void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st);
 void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st);
 
 // ---- fused gradient -> normalise -> divergence (face.cu) ----

@@ -286,6 +286,55 @@ int build_symbolic(const MeshPrep& m, int leaf_size, int max_width, int relax, S
             ++j;
         }
     }
+    // 4b. amalgamation: merge a supernode into its parent when their columns are
+    // contiguous and the explicit zeros stay small (fewer, wider supernodes and
+    // fewer etree levels). For a supernode whose columns form an etree chain or
+    // subtree, its row structure beyond its last column l has colcount[l]-1 rows.
+    {
+        const int32_t n0 = (int32_t)S.sn_c0.size();
+        std::vector<int32_t> first(S.sn_c0.begin(), S.sn_c0.end());
+        std::vector<int32_t> last(n0);
+        for (int32_t s = 0; s < n0; ++s) last[s] = (s + 1 < n0 ? S.sn_c0[s + 1] : (int32_t)n) - 1;
+        std::vector<double> truenz(n0, 0.0);
+        for (int32_t s = 0; s < n0; ++s)
+            for (int32_t j = first[s]; j <= last[s]; ++j) truenz[s] += (double)colcount[j];
+        std::vector<int32_t> into(n0, -1);
+        auto find = [&](int32_t s) {
+            while (into[s] != -1) s = into[s];
+            return s;
+        };
+        for (int pass = 0; pass < 8; ++pass) {
+            bool changed = false;
+            for (int32_t s = 0; s < n0; ++s) {
+                if (into[s] != -1) continue;
+                const int32_t pc = parent[last[s]];
+                if (pc == -1) continue;
+                const int32_t p = find(S.col_sn[pc]);
+                if (last[s] + 1 != first[p]) continue;
+                const double nsm = (double)(last[p] - first[s] + 1);
+                if (nsm > max_width) continue;
+                const double nrp = (double)(colcount[last[p]] - 1);
+                const double stored = nsm * (nsm + 1.0) / 2.0 + nsm * nrp;
+                const double zf = 1.0 - (truenz[s] + truenz[p]) / stored;
+                const bool ok = nsm <= 4 || (nsm <= 16 && zf < 0.8) || (nsm <= 48 && zf < 0.1) || zf < 0.05;
+                if (!ok) continue;
+                first[p] = first[s];
+                truenz[p] += truenz[s];
+                into[s] = p;
+                changed = true;
+            }
+            if (!changed) break;
+        }
+        std::vector<int32_t> c0;
+        for (int32_t s = 0; s < n0; ++s)
+            if (into[s] == -1) c0.push_back(first[s]);
+        std::sort(c0.begin(), c0.end());
+        S.sn_c0 = c0;
+        for (size_t s = 0; s < c0.size(); ++s) {
+            const int32_t e = s + 1 < c0.size() ? c0[s + 1] : (int32_t)n;
+            for (int32_t j = c0[s]; j < e; ++j) S.col_sn[j] = (int32_t)s;
+        }
+    }
     const int32_t ns_total = (int32_t)S.sn_c0.size();
     S.nsuper = ns_total;
     S.sn_c0.push_back((int32_t)n);

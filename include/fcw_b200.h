@@ -42,7 +42,7 @@ enum {
 typedef struct fcw_params {
     double diffusion_length_mm; /* sqrt(t) in mm; >= 0.5 (distance_engines.py:82-89) */
     double poisson_shift;       /* Poisson regulariser: L + shift*M (fastcw_lean.py:481, 500) */
-    int32_t block_k;            /* sources per right-hand-side block, a multiple of 32 */
+    int32_t block_k;            /* sources per right-hand-side block, a multiple of 64 */
     int32_t leaf_size;          /* nested-dissection leaf size */
     int32_t max_width;          /* widest supernode (columns), <= 64 */
     int32_t relax;              /* etree subtrees of at most this many columns become one supernode */

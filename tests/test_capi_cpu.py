@@ -26,7 +26,7 @@ def test_library_loads_and_exports_every_declared_symbol():
 def test_params_struct_matches_defaults():
     p = _lib.default_params()
     assert p.diffusion_length_mm == 0.7 and p.poisson_shift == 1e-10
-    assert p.block_k % 32 == 0 and 1 <= p.relax <= p.max_width <= 64
+    assert p.block_k % 64 == 0 and 1 <= p.relax <= p.max_width <= 64
     assert _lib.metrics_stride(12, 3) == 7 + 24 + 66
 
 

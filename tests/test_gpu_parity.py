@@ -131,7 +131,7 @@ def test_geometry_on_reference_fields(l4):
 def test_geometry_kat_fields_long_faces_and_nan_rules():
     z = dict(np.load(os.path.join(GOLDEN, "golden_geometry_kat.npz")))
     V, F = z["V"], z["F"].astype(np.int32)
-    eng = engine.HeatEngine(V, F, block_k=32)
+    eng = engine.HeatEngine(V, F, block_k=64)
     try:
         fields = z["fields"][[0, 3]]
         # the euclid stub field is healthy; the perturbed one exercises the long-face list.
@@ -181,3 +181,21 @@ def test_l5_metrics_match_reference_float32_outputs(precision, tol):
         assert np.max(_rel(r["radii"][:, i], z["f32_radius_" + tok])) <= max(tol, 2.4e-7)
         assert np.max(_rel(r["perim"][:, i], z["f32_perimeter_" + tok])) <= max(tol, 2.4e-7)
     assert np.max(_rel(r["msd_u"], z["f32_msd_unweighted"])) <= max(tol / 10, 2.4e-7)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 2e-5)])
+def test_full_blocks_every_column_tile(precision, tol):
+    """256-source blocks (four 64-column tiles, multi-chunk supernodes) against the oracle."""
+    import oracle
+    z = _golden("golden_metrics_L5.npz")
+    pm = z["pm"]
+    src = pm.bfs[np.linspace(0, pm.n_vertices - 1, 256).astype(int)]
+    cols = [0, 63, 64, 100, 128, 191, 192, 255]
+    ref = oracle.HeatOracle(pm.V, pm.F).distances(src[cols])
+    eng = engine.HeatEngine(pm.V, pm.F, block_k=256)
+    try:
+        d = eng.compute_distances(src, precision=precision)[cols]
+    finally:
+        eng.close()
+    err = np.max(np.abs(d - ref), axis=1) / np.max(np.abs(ref), axis=1)
+    assert np.max(err) <= tol, err
