@@ -231,10 +231,8 @@ def _stage_bytes(stage, n, nf, K, nnz_factor, precision, nreached_rows=None):
         return n * K * 8 + n * K * b + nf * (3 * 4 + 4 * 4) + 3 * nf * 5
     if stage == "shift":
         return 2 * n * K * b
-    if stage == "vertex_stats":
+    if stage == "metrics":
         return n * K * b + n * 32
-    if stage == "geometry":
-        return n * K * b + nf * (12 + 32)
     if stage == "heat_fwd":
         return nnz_factor * 8
     return 0
@@ -459,8 +457,8 @@ def main(argv=None):
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="L7")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--batch", type=int, default=2048, help="sources per step")
-    ap.add_argument("--block-k", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=4096, help="sources per step")
+    ap.add_argument("--block-k", type=int, default=1024)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=24, help="sources timed on the CPU oracle (0 = skip)")

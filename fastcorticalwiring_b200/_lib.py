@@ -27,7 +27,7 @@ EXPORTED = (
     "fcw_heat_solve_device", "fcw_divergence_device", "fcw_poisson_solve_device", "fcw_field_metrics_device",
     "fcw_engine_profile", "fcw_engine_stage_times",
 )
-STAGES = ("heat_fwd", "heat_bwd", "divergence", "poisson_fwd", "poisson_bwd", "shift", "vertex_stats", "geometry")
+STAGES = ("heat_fwd", "heat_bwd", "divergence", "poisson_fwd", "poisson_bwd", "shift", "metrics")
 
 
 class FCWParams(ctypes.Structure):

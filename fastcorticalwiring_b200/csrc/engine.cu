@@ -57,13 +57,13 @@ __global__ void k_map_sources(int64_t n, const int32_t* __restrict__ sources, co
     out[k] = v;
 }
 
-// d (k rows, caller vertex order) -> dT (K rows, elimination order); rows >= k are zero.
+// d (k rows, caller vertex order) -> Y (n x K vertex-major, elimination order); columns >= k are zero.
 __global__ void k_fields_in(int32_t n, int32_t k, int32_t K, const double* __restrict__ d,
-                            const int32_t* __restrict__ iperm, double* __restrict__ dT) {
+                            const int32_t* __restrict__ iperm, double* __restrict__ Y) {
     const int64_t total = (int64_t)K * n;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
         const int r = (int)(e / n), i = (int)(e - (int64_t)r * n);
-        if (r < k) dT[(int64_t)r * n + iperm[i]] = d[e];
+        Y[(int64_t)iperm[i] * K + r] = r < k ? d[(int64_t)r * n + i] : 0.0;
     }
 }
 
@@ -84,6 +84,9 @@ struct Workspace {
     double* out = nullptr;
     int32_t out_stride = 0;
     double* U = nullptr;        // forward update rows, (sum nr) x K doubles (reused as floats)
+    double* partials = nullptr; // per (vertex tile, source) health/MSD partial sums
+    int32_t* near_list = nullptr;
+    int32_t* near_count = nullptr;
     double* part = nullptr;     // backward split-K partial sums
     int* counters = nullptr;    // split-K arrival tickets, zero at rest
 };
@@ -119,6 +122,7 @@ struct fcw_engine {
     int* err_d = nullptr;
     Workspace ws;
     double analyze_ms = 0.0, factor_ms = 0.0;
+    double lean_total = 0.0;  // sum of the lean face areas (the prefix total of a finite field)
     // stage timeline (CUDA events on the working stream), off unless enabled
     bool prof_on = false;
     std::vector<std::pair<int, cudaEvent_t>> marks;
@@ -434,6 +438,8 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     FCW_TRY(e->upload(&e->varea_d, varea));
     FCW_TRY(e->upload(&e->boundary_d, bnd));
     FCW_TRY(e->upload(&e->farea_d, m.lean_area));
+    e->lean_total = 0.0;
+    for (double x : m.lean_area) e->lean_total += x;
     FCW_TRY(e->upload(&e->g11_d, m.g11));
     FCW_TRY(e->upload(&e->g12_d, m.g12));
     FCW_TRY(e->upload(&e->g22_d, m.g22));
@@ -493,7 +499,7 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
     const int32_t Kn = std::max(K, w.K);
     const int32_t sn = std::max(stride, w.out_stride);
     void* old[] = {w.Bh, w.Bp64, w.Bp32, w.Y, w.dT64, w.dT32, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
-                   w.counters};
+                   w.counters, w.partials, w.near_list, w.near_count};
     for (void* p : old)
         if (p) e->release(p);
     w = Workspace{};
@@ -509,6 +515,10 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
     FCW_TRY(e->dalloc(&w.band, (size_t)nf * Kn));
     FCW_TRY(e->dalloc(&w.longf, (size_t)nf * Kn));
     FCW_TRY(e->dalloc(&w.out, (size_t)sn * Kn));
+    const int64_t ntiles = (n + fcw::kStatVTile - 1) / fcw::kStatVTile;
+    FCW_TRY(e->dalloc(&w.partials, (size_t)ntiles * Kn * 8));
+    FCW_TRY(e->dalloc(&w.near_list, (size_t)n * Kn));
+    FCW_TRY(e->dalloc(&w.near_count, (size_t)Kn));
     FCW_TRY(e->dalloc(&w.U, (size_t)std::max<int64_t>(e->n_urows, 1) * Kn));
     FCW_TRY(e->dalloc(&w.part, (size_t)std::max<int64_t>(e->n_parts, 1) * fcw::kMaxWidth * Kn));
     const int64_t nctr = (int64_t)std::max<int32_t>(e->sym.nsuper, 1) * (Kn / fcw::kRhsTile);
@@ -578,7 +588,8 @@ void poisson_solve(fcw_engine* e, const T* val, const T* inv, const T* R, T* Y, 
 }
 
 // Distances for the K sources in ws.src, shifted, source-major in ws.dT64 / ws.dT32.
-void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st) {
+// With metric arguments, the shift also produces the health/MSD partials and near lists.
+void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, const fcw::MetricArgs* ma = nullptr) {
     Workspace& w = e->ws;
     const int32_t n = (int32_t)e->sym.n;
     heat_solve(e, K, st);
@@ -588,12 +599,14 @@ void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st) {
         fcw::launch_divergence_mixed(e->fd, w.Bh, w.Bp32, K, e->ground_new, st);
         poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, Y, K, st);
         mark(e, st, FCW_STAGE_SHIFT);
-        fcw::launch_shift_transpose<float, float>(n, K, Y, w.src, w.dT32, st);
+        if (ma) fcw::launch_shift_stats<float, float>(*ma, K, Y, w.dT32, st);
+        else fcw::launch_shift_transpose<float, float>(n, K, Y, w.src, w.dT32, st);
     } else {
         fcw::launch_divergence_fp64(e->fd, w.Bh, w.Bp64, K, st);
         poisson_solve<double>(e, e->val_p, e->inv_p, w.Bp64, w.Y, K, st);
         mark(e, st, FCW_STAGE_SHIFT);
-        fcw::launch_shift_transpose<double, double>(n, K, w.Y, w.src, w.dT64, st);
+        if (ma) fcw::launch_shift_stats<double, double>(*ma, K, w.Y, w.dT64, st);
+        else fcw::launch_shift_transpose<double, double>(n, K, w.Y, w.src, w.dT64, st);
     }
     e->launches += 2;
 }
@@ -617,6 +630,10 @@ int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, do
     a.vertex_area = e->varea_d;
     a.boundary = e->boundary_d;
     a.fv = e->fd.fv;
+    a.inc_ptr = e->fd.inc_ptr;
+    a.inc_face = e->fd.inc_face;
+    a.inc_corner = e->fd.inc_corner;
+    a.total_area = e->lean_total;
     a.farea = e->farea_d;
     a.g11 = e->g11_d;
     a.g12 = e->g12_d;
@@ -628,6 +645,20 @@ int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, do
     a.max_iter = 60;
     for (int32_t i = 0; i < nt; ++i) a.targets[i] = targets[i];
     for (int32_t j = 0; j < nb; ++j) a.fracs[j] = (double)(j + 1) / ((double)nb + 1.0);
+    a.K = nsrc;
+    a.ntiles = (int32_t)((e->sym.n + fcw::kStatVTile - 1) / fcw::kStatVTile);
+    a.partials = e->ws.partials;
+    a.near_list = e->ws.near_list;
+    a.near_count = e->ws.near_count;
+    {
+        // near radius: a flat disc holding twice the largest reachable target, in whole bins
+        double tmax = 0.0;
+        for (int32_t i = 0; i < nt; ++i)
+            if (targets[i] > tmax && targets[i] <= e->lean_total) tmax = targets[i];
+        const double r0 = std::sqrt(2.0 * tmax / 3.141592653589793);
+        a.near_bins = (int32_t)std::ceil(r0 / e->mesh.bin_width) + 2;
+        a.near_radius = (double)a.near_bins * e->mesh.bin_width;
+    }
     a.src = e->ws.src;
     a.band = e->ws.band;
     a.longf = e->ws.longf;
@@ -638,12 +669,10 @@ int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, do
 
 template <typename T>
 void metrics_block(fcw_engine* e, fcw::MetricArgs& a, const T* dT, cudaStream_t st) {
-    mark(e, st, FCW_STAGE_VERTEX_STATS);
-    fcw::launch_vertex_stats<T>(a, dT, st);
-    mark(e, st, FCW_STAGE_GEOMETRY);
-    fcw::launch_geometry<T>(a, dT, st);
+    mark(e, st, FCW_STAGE_METRICS);
+    fcw::launch_source_metrics<T>(a, dT, st);
     mark(e, st, -1);
-    e->launches += 2;
+    e->launches += 1;
 }
 
 int check_engine(fcw_engine* e) {
@@ -680,7 +709,7 @@ void fcw_default_params(fcw_params* p) {
     if (!p) return;
     p->diffusion_length_mm = 0.7;
     p->poisson_shift = 1e-10;
-    p->block_k = 256;
+    p->block_k = 1024;
     p->leaf_size = 64;
     p->max_width = 64;
     p->relax = 32;
@@ -871,7 +900,7 @@ int fcw_compute_metrics(fcw_engine* e, const int32_t* sources, int64_t n, int32_
         fcw::MetricArgs a;
         FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
         FCW_TRY(map_sources_host(e, sources + b0, nbk, K, e->stream, buf));
-        distances_block(e, K, precision, e->stream);
+        distances_block(e, K, precision, e->stream, &a);
         if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, e->ws.dT32, e->stream);
         else metrics_block<double>(e, a, e->ws.dT64, e->stream);
         FCW_CUDA(cudaGetLastError());
@@ -901,7 +930,7 @@ int fcw_compute_metrics_device(fcw_engine* e, const int32_t* sources_dev, int64_
         k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(nbk, sources_dev + b0, e->iperm_d, (int32_t)e->sym.n, K,
                                                        e->ws.src, e->err_d);
         e->launches += 1;
-        distances_block(e, K, precision, st);
+        distances_block(e, K, precision, st, &a);
         if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, e->ws.dT32, st);
         else metrics_block<double>(e, a, e->ws.dT64, st);
         FCW_CUDA(cudaGetLastError());
@@ -996,7 +1025,8 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
     a.out = out_dev;
     k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->ws.src,
                                                    e->err_d);
-    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)e->sym.n, k, K, d_dev, e->iperm_d, e->ws.dT64);
+    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)e->sym.n, k, K, d_dev, e->iperm_d, e->ws.Y);
+    fcw::launch_shift_stats<double, double>(a, K, e->ws.Y, e->ws.dT64, st);
     metrics_block<double>(e, a, e->ws.dT64, st);
     FCW_CUDA(cudaGetLastError());
     return FCW_OK;

@@ -117,6 +117,10 @@ struct MetricArgs {
     const double* vertex_area = nullptr;
     const int32_t* boundary = nullptr;  // elimination-order ids
     const int32_t* fv = nullptr;
+    const int32_t* inc_ptr = nullptr;   // vertex -> incident faces (elimination order)
+    const int32_t* inc_face = nullptr;
+    const int8_t* inc_corner = nullptr;
+    double total_area = 0.0;            // sum of the lean face areas
     const double* farea = nullptr;      // lean face area, g11, g12, g22 (lean_geometry.py:44-63)
     const double* g11 = nullptr;
     const double* g12 = nullptr;
@@ -126,14 +130,26 @@ struct MetricArgs {
     double targets[kMaxTargets];
     double fracs[kMaxBetween];
     const int32_t* src = nullptr;       // elimination-order source per column
-    int32_t* band = nullptr;            // nsrc * nf scratch
-    int32_t* longf = nullptr;           // nsrc * nf scratch
+    int32_t* band = nullptr;            // nsrc * nf scratch: near faces sorted by bin
+    int32_t* longf = nullptr;           // nsrc * nf scratch: near long faces
     double* out = nullptr;              // nsrc * stride
     int* err = nullptr;
+    // shift + statistics (k_shift_stats) -> per-source kernel
+    int32_t K = 0;                      // columns of the block (partials' leading dimension)
+    int32_t ntiles = 0;                 // vertex tiles of kStatVTile vertices
+    double* partials = nullptr;         // ntiles x K x 8 partial statistics
+    double near_radius = 0.0;           // = near_bins * width
+    int32_t near_bins = 0;
+    int32_t* near_list = nullptr;       // K x n: vertices closer than near_radius, per source
+    int32_t* near_count = nullptr;      // K
 };
+constexpr int kStatVTile = 256;   // vertices per shift-statistics CTA
+// phi (n x K) -> dT (K x n) with phi[source] subtracted, plus per-tile health/MSD
+// partials and the per-source near-vertex lists.
+template <typename Tin, typename Tout>
+void launch_shift_stats(const MetricArgs& a, int32_t K, const Tin* phi, Tout* dT, cudaStream_t st);
+// Health, MSD, distance to boundary, radii, perimeters and samples of each source's field.
 template <typename T>
-void launch_vertex_stats(const MetricArgs& a, const T* dT, cudaStream_t st);
-template <typename T>
-void launch_geometry(const MetricArgs& a, const T* dT, cudaStream_t st);
+void launch_source_metrics(const MetricArgs& a, const T* dT, cudaStream_t st);
 
 }  // namespace fcw

@@ -1,18 +1,11 @@
-// Per-source kernels: shift + transpose, vertex statistics, radius/perimeter geometry.
+// Per-source kernels: shift + transpose, then all per-source metrics.
 //
 // After the Poisson solve the fields sit in an n x K vertex-major block. The
 // shift kernel subtracts each column's value at its source and transposes to
-// K x n (one contiguous field per source), which the per-source kernels read:
-//
-//  * vertex statistics, one CTA per source: health screen (lean_geometry.py:343-357),
-//    MSD unweighted/area-weighted and distance to boundary (core_analysis.py:1566-1581);
-//  * geometry, one CTA per source (lean_geometry.py:117-340): faces are binned by
-//    their largest distance into bins of fixed width; the area histogram's
-//    prefix sums bracket every target area, faces in the bracketing bins are
-//    compacted once (counting sort by bin), and one warp per target runs the
-//    reference's safeguarded Newton iteration on A(r) with the exact
-//    piecewise-quadratic face areas, then the coarea perimeter; the
-//    supplementary log-spaced samples follow, one warp per sample.
+// K x n (one contiguous field per source). k_source_metrics then computes, one
+// CTA per source, the health screen, MSD, distance to boundary, and the
+// radius/perimeter geometry of lean_geometry.py restricted to the faces near
+// the source (see its comment for why that restriction is exact).
 #include <math.h>
 
 #include "kernels.cuh"
@@ -43,80 +36,123 @@ __global__ void k_shift_transpose(int32_t n, int32_t K, const Tin* __restrict__ 
     }
 }
 
+
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_vertex_stats(MetricArgs a, const T* __restrict__ dT) {
-    const int k = blockIdx.x;
-    const int s = a.src[k];
-    if (s < 0) return;
-    const T* d = dT + (int64_t)k * a.n;
-    const double xs0 = a.coords[3 * (int64_t)s], xs1 = a.coords[3 * (int64_t)s + 1], xs2 = a.coords[3 * (int64_t)s + 2];
-    const double h = a.health_h;
-    double sum_d = 0.0, sum_da = 0.0, sum_a = 0.0;
-    int cnt = 0, neg = 0, viol = 0, nonfinite = 0;
-    for (int i = threadIdx.x; i < a.n; i += blockDim.x) {
-        const double di = (double)d[i];
-        if (!isfinite(di)) { ++nonfinite; continue; }
-        if (di < -h) ++neg;
-        const double dx = a.coords[3 * (int64_t)i] - xs0;
-        const double dy = a.coords[3 * (int64_t)i + 1] - xs1;
-        const double dz = a.coords[3 * (int64_t)i + 2] - xs2;
-        const double chord = __dsqrt_rn(dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz)));
-        if (di < __dsub_rn(dmul(0.9, chord), h)) ++viol;
-        if (di > a.eps) {
-            const double w = a.vertex_area[i];
-            sum_d += di;
-            sum_da += di * w;
-            sum_a += w;
-            ++cnt;
+// Per-(vertex tile, source) partial statistics written by k_shift_stats.
+enum { P_SUM_D, P_SUM_DA, P_SUM_A, P_CNT, P_NEG, P_VIOL, P_NONFINITE, P_DMAX, P_N };
+
+// The shift + transpose of one 256-vertex x 32-source tile, fused with the per-vertex
+// work of the health screen and MSD (lean_geometry.py:343-357, core_analysis.py:1573-1581):
+// counts of d < -h and of d < 0.9 |x - x_s| - h, the valid-distance sums and the maximum.
+// The chord test compares squares and takes the reference's sqrt form only within a
+// 1e-10 band of the threshold, so the counts match the reference exactly. Vertices
+// closer than the near radius are appended to their source's near list.
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(256) k_shift_stats(MetricArgs a, int32_t K, const Tin* __restrict__ phi,
+                                                     Tout* __restrict__ dT) {
+    __shared__ Tin tile[32][33];
+    __shared__ Tin sh[32];
+    __shared__ double sc[32][3];
+    __shared__ double vc[32][4];
+    __shared__ int srcv[32];
+    const int n = a.n;
+    const int k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    if (ty == 0) {
+        const int sidx = a.src[k0 + tx];
+        srcv[tx] = sidx;
+        sh[tx] = sidx >= 0 ? phi[(int64_t)sidx * K + k0 + tx] : Tin(0);
+        for (int c = 0; c < 3; ++c) sc[tx][c] = sidx >= 0 ? a.coords[3 * (int64_t)sidx + c] : 0.0;
+    }
+    double sd[4], sda[4], sa[4], dm[4];
+    int cnt[4], ng[4], vi[4], nf[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) { sd[j] = sda[j] = sa[j] = 0.0; dm[j] = 0.0; cnt[j] = ng[j] = vi[j] = nf[j] = 0; }
+    const double h = a.health_h, R0 = a.near_radius;
+    const unsigned lanes_below = (1u << tx) - 1u;
+    for (int sub = 0; sub < kStatVTile / 32; ++sub) {
+        const int v0 = blockIdx.x * kStatVTile + sub * 32;
+        if (v0 >= n) break;
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int v = v0 + r;
+            tile[r][tx] = v < n ? phi[(int64_t)v * K + k0 + tx] : Tin(0);
+        }
+        if (ty == 0 && v0 + tx < n) {
+            const int v = v0 + tx;
+            for (int c = 0; c < 3; ++c) vc[tx][c] = a.coords[3 * (int64_t)v + c];
+            vc[tx][3] = a.vertex_area[v];
+        }
+        __syncthreads();
+        const int v = v0 + tx;
+        const bool in = v < n;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = ty + 8 * j, k = k0 + r;
+            const Tout dv = (Tout)(tile[tx][r] - sh[r]);
+            if (in) dT[(int64_t)k * n + v] = dv;
+            if (srcv[r] < 0) continue;  // warp-uniform (one source per warp)
+            const double di = (double)dv;
+            bool near = false;
+            if (in) {
+                if (!isfinite(di)) {
+                    ++nf[j];
+                } else {
+                    if (di < -h) ++ng[j];
+                    const double dx = vc[tx][0] - sc[r][0], dy = vc[tx][1] - sc[r][1], dz = vc[tx][2] - sc[r][2];
+                    const double c2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+                    const double t = di + h;
+                    bool viol;
+                    if (t < 0.0) {
+                        viol = true;
+                    } else {
+                        const double lhs = t * t, rhs = 0.81 * c2;
+                        if (lhs < rhs * (1.0 - 1e-10)) viol = true;
+                        else if (lhs > rhs * (1.0 + 1e-10)) viol = false;
+                        else viol = di < __dsub_rn(dmul(0.9, __dsqrt_rn(c2)), h);
+                    }
+                    if (viol) ++vi[j];
+                    if (di > a.eps) {
+                        const double wa = vc[tx][3];
+                        sd[j] += di;
+                        sda[j] += di * wa;
+                        sa[j] += wa;
+                        ++cnt[j];
+                    }
+                    dm[j] = fmax(dm[j], di);
+                    near = di < R0;
+                }
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, near);
+            if (mask) {
+                int base = 0;
+                if (tx == 0) base = atomicAdd(&a.near_count[k], __popc(mask));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (near) a.near_list[(int64_t)k * n + base + __popc(mask & lanes_below)] = v;
+            }
         }
     }
-    double bmin = INFINITY;
-    int bcnt = 0;
-    for (int i = threadIdx.x; i < a.n_boundary; i += blockDim.x) {
-        const double di = (double)d[a.boundary[i]];
-        if (isfinite(di)) { bmin = fmin(bmin, di); ++bcnt; }
-    }
-    // block reduction
-    __shared__ double rd[4][8];
-    __shared__ int ri[5][8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) {
-        sum_d += __shfl_down_sync(0xffffffffu, sum_d, o);
-        sum_da += __shfl_down_sync(0xffffffffu, sum_da, o);
-        sum_a += __shfl_down_sync(0xffffffffu, sum_a, o);
-        bmin = fmin(bmin, __shfl_down_sync(0xffffffffu, bmin, o));
-        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-        neg += __shfl_down_sync(0xffffffffu, neg, o);
-        viol += __shfl_down_sync(0xffffffffu, viol, o);
-        nonfinite += __shfl_down_sync(0xffffffffu, nonfinite, o);
-        bcnt += __shfl_down_sync(0xffffffffu, bcnt, o);
-    }
-    if (lane == 0) {
-        rd[0][warp] = sum_d; rd[1][warp] = sum_da; rd[2][warp] = sum_a; rd[3][warp] = bmin;
-        ri[0][warp] = cnt; ri[1][warp] = neg; ri[2][warp] = viol; ri[3][warp] = nonfinite; ri[4][warp] = bcnt;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int nw = blockDim.x >> 5;
-        double Sd = 0, Sda = 0, Sa = 0, Bm = INFINITY;
-        int C = 0, NG = 0, VI = 0, NF = 0, BC = 0;
-        for (int w = 0; w < nw; ++w) {
-            Sd += rd[0][w]; Sda += rd[1][w]; Sa += rd[2][w]; Bm = fmin(Bm, rd[3][w]);
-            C += ri[0][w]; NG += ri[1][w]; VI += ri[2][w]; NF += ri[3][w]; BC += ri[4][w];
+    // reduce over the 32 vertices of each warp (lanes), one source per (warp, j)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        for (int off = 16; off > 0; off >>= 1) {
+            sd[j] += __shfl_down_sync(0xffffffffu, sd[j], off);
+            sda[j] += __shfl_down_sync(0xffffffffu, sda[j], off);
+            sa[j] += __shfl_down_sync(0xffffffffu, sa[j], off);
+            dm[j] = fmax(dm[j], __shfl_down_sync(0xffffffffu, dm[j], off));
+            cnt[j] += __shfl_down_sync(0xffffffffu, cnt[j], off);
+            ng[j] += __shfl_down_sync(0xffffffffu, ng[j], off);
+            vi[j] += __shfl_down_sync(0xffffffffu, vi[j], off);
+            nf[j] += __shfl_down_sync(0xffffffffu, nf[j], off);
         }
-        double* o = a.out + (int64_t)k * a.stride;
-        const double nan = __longlong_as_double(0x7ff8000000000000LL);
-        o[0] = C > 0 ? Sd / (double)C : nan;
-        o[1] = (C > 0 && isfinite(Sa) && Sa > 0.0) ? Sda / Sa : nan;
-        o[2] = a.n_boundary > 0 ? (BC > 0 ? Bm : nan) : INFINITY;
-        const double negf = NF ? nan : (double)NG / (double)a.n;
-        const double violf = NF ? nan : (double)VI / (double)a.n;
-        o[3] = negf;
-        o[4] = violf;
-        o[5] = (NF > 0 || negf > 1e-3 || violf > 1e-3) ? 1.0 : 0.0;
+        if (tx == 0) {
+            const int k = k0 + ty + 8 * j;
+            double* q = a.partials + ((int64_t)blockIdx.x * K + k) * P_N;
+            q[P_SUM_D] = sd[j]; q[P_SUM_DA] = sda[j]; q[P_SUM_A] = sa[j]; q[P_CNT] = (double)cnt[j];
+            q[P_NEG] = (double)ng[j]; q[P_VIOL] = (double)vi[j]; q[P_NONFINITE] = (double)nf[j]; q[P_DMAX] = dm[j];
+        }
     }
 }
 
@@ -160,42 +196,55 @@ __device__ __forceinline__ double warp_sum(double v) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
-struct GeoShared {
-    double pre[kMaxBins];   // exclusive prefix of face area per bin
-    int ptr[kMaxBins];      // exclusive prefix of face count per bin
+struct SrcShared {
+    double pre[kMaxBins + 1];  // vertex-area histogram (fixed point) first, then face-area prefix sums
+    int ptr[kMaxBins + 1];     // faces per bin -> exclusive prefix
     int fill[kMaxBins];
-    double red[32];
+    double red[16][4];
+    double dred[16][5];
     double radii[kMaxTargets];
-    double total;
-    int nbins, nlong, ntot, b_lo, b_hi, base, n_eval, bad_scan;
+    double total, dglob;
+    int nbins, rc, nlong, ntot, n_eval, bad, overflow;
 };
 
+// A source's distance field with its near-face bins (lean_geometry.py:117-299 restated over
+// the faces that can matter): bins [0, rc) are complete, larger bins are never queried.
 template <typename T>
 struct Field {
     const T* d;
     const MetricArgs* a;
-    GeoShared* s;
-    const int32_t* band;   // compacted faces of bins [b_lo, b_hi], sorted by bin
-    const int32_t* longf;
+    SrcShared* s;
+    const int32_t* band;   // near faces sorted by bin
+    const int32_t* longf;  // near faces whose distance extent exceeds the bin width
 
     __device__ double dv(int v) const { return (double)d[v]; }
     __device__ int bin_of(double dmax) const {
-        int k = (int)(dmax / a->width);
+        const int k = (int)(dmax / a->width);
         return k < 0 ? 0 : k;
     }
-    __device__ int ptr_at(int k) const { return k < s->nbins ? s->ptr[k] : s->ntot; }
-    __device__ double prefix_at(int k) const { return k < s->nbins ? s->pre[k] : s->total; }
+    __device__ double prefix_at(int k) const { return k <= s->rc && k < s->nbins ? s->pre[k] : s->total; }
 
-    // Band + long-face sums over faces with bin in [kr, kend), all lanes of a warp.
-    // mode 0: (A, dA) contributions; mode 1: perimeter.
+    __device__ void face_term(int f, double r, int mode, double& x1, double& x2) const {
+        const int* fv = a->fv;
+        const double d0 = dv(fv[3 * f]), d1 = dv(fv[3 * f + 1]), d2 = dv(fv[3 * f + 2]);
+        double ar, da;
+        face_cdf(d0, d1, d2, a->farea[f], r, ar, da);
+        if (mode == 0) {
+            x1 += ar;
+            x2 += da;
+        } else if (da > 0.0) {
+            x1 += da * grad_norm(d0, d1, d2, a->g11[f], a->g12[f], a->g22[f]);
+        }
+    }
+
+    // Faces with bin in [kr, kend) plus long faces with bin >= kend, summed by one warp.
     __device__ void band_sum(int kr, int kend, double r, int mode, double& s1, double& s2) const {
         const int lane = threadIdx.x & 31;
         double x1 = 0.0, x2 = 0.0;
         const int* fv = a->fv;
-        if (kr >= s->b_lo && kend - 1 <= s->b_hi) {
-            const int j0 = ptr_at(kr) - s->base, j1 = ptr_at(kend) - s->base;
-            for (int j = j0 + lane; j < j1; j += 32) face_term(band[j], r, mode, x1, x2);
-        } else {  // outside the compacted range: scan every face (rare; long-face walk-down)
+        if (kend <= s->rc) {
+            for (int j = s->ptr[kr] + lane; j < s->ptr[kend]; j += 32) face_term(band[j], r, mode, x1, x2);
+        } else {  // beyond the complete bins: scan every face (not reached for healthy fields)
             for (int f = lane; f < a->nf; f += 32) {
                 const double d0 = dv(fv[3 * f]), d1 = dv(fv[3 * f + 1]), d2 = dv(fv[3 * f + 2]);
                 if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
@@ -210,19 +259,6 @@ struct Field {
         }
         s1 = warp_sum(x1);
         s2 = warp_sum(x2);
-    }
-
-    __device__ void face_term(int f, double r, int mode, double& x1, double& x2) const {
-        const int* fv = a->fv;
-        const double d0 = dv(fv[3 * f]), d1 = dv(fv[3 * f + 1]), d2 = dv(fv[3 * f + 2]);
-        double ar, da;
-        face_cdf(d0, d1, d2, a->farea[f], r, ar, da);
-        if (mode == 0) {
-            x1 += ar;
-            x2 += da;
-        } else if (da > 0.0) {
-            x1 += da * grad_norm(d0, d1, d2, a->g11[f], a->g12[f], a->g22[f]);
-        }
     }
 
     // lean_geometry.py:183-212
@@ -248,7 +284,7 @@ struct Field {
         return b1;
     }
 
-    // lean_geometry.py:247-299 (bracket already known: lo_i)
+    // lean_geometry.py:247-299
     __device__ double solve_radius(double target, int& n_eval) const {
         n_eval = 0;
         const double nan = __longlong_as_double(0x7ff8000000000000LL);
@@ -293,9 +329,20 @@ struct Field {
     }
 };
 
+
+// Everything computed from one source's field, one CTA per source:
+//   1. the health screen, MSD and global max from the shift kernel's partial sums,
+//      and the distance to boundary;
+//   2. the faces that have a corner closer than rc*w (rc starts at the near radius
+//      of the shift kernel's near lists), each emitted once by its first near corner
+//      through the vertex->face incidence lists: their area histogram, counting sort
+//      by bin and the long-face list (lean_geometry.py:117-180 on these faces). Bins
+//      below rc are complete. If the largest target is not enclosed two bins below rc,
+//      rc grows (up to every bin, scanning all vertices) and step 2 repeats;
+//   3. one warp per target: bracket + safeguarded Newton + perimeter; then the samples.
 template <typename T>
-__global__ void __launch_bounds__(512) k_geometry(MetricArgs a, const T* __restrict__ dT) {
-    __shared__ GeoShared S;
+__global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
+    __shared__ SrcShared S;
     const int k = blockIdx.x;
     const int src = a.src[k];
     if (src < 0) return;
@@ -308,120 +355,173 @@ __global__ void __launch_bounds__(512) k_geometry(MetricArgs a, const T* __restr
     const T* d = dT + (int64_t)k * a.n;
     int32_t* band = a.band + (int64_t)k * a.nf;
     int32_t* longf = a.longf + (int64_t)k * a.nf;
+    const double w = a.width;
 
+    // 1. reduce the shift kernel's partial statistics (fixed order: deterministic)
+    double sum_d = 0.0, sum_da = 0.0, sum_a = 0.0, dmax = 0.0;
+    double cnt = 0.0, neg = 0.0, viol = 0.0, nonfinite = 0.0;
+    for (int tI = tid; tI < a.ntiles; tI += bs) {
+        const double* q = a.partials + ((int64_t)tI * a.K + k) * P_N;
+        sum_d += q[P_SUM_D]; sum_da += q[P_SUM_DA]; sum_a += q[P_SUM_A]; cnt += q[P_CNT];
+        neg += q[P_NEG]; viol += q[P_VIOL]; nonfinite += q[P_NONFINITE]; dmax = fmax(dmax, q[P_DMAX]);
+    }
+    double bmin = INFINITY;
+    double bcnt = 0.0;
+    for (int i = tid; i < a.n_boundary; i += bs) {
+        const double di = (double)d[a.boundary[i]];
+        if (isfinite(di)) { bmin = fmin(bmin, di); bcnt += 1.0; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sum_d += __shfl_down_sync(0xffffffffu, sum_d, off);
+        sum_da += __shfl_down_sync(0xffffffffu, sum_da, off);
+        sum_a += __shfl_down_sync(0xffffffffu, sum_a, off);
+        bmin = fmin(bmin, __shfl_down_sync(0xffffffffu, bmin, off));
+        dmax = fmax(dmax, __shfl_down_sync(0xffffffffu, dmax, off));
+        cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+        neg += __shfl_down_sync(0xffffffffu, neg, off);
+        viol += __shfl_down_sync(0xffffffffu, viol, off);
+        nonfinite += __shfl_down_sync(0xffffffffu, nonfinite, off);
+        bcnt += __shfl_down_sync(0xffffffffu, bcnt, off);
+    }
+    if (lane == 0) {
+        S.red[warp][0] = sum_d; S.red[warp][1] = sum_da; S.red[warp][2] = sum_a; S.red[warp][3] = bmin;
+        S.dred[warp][0] = cnt; S.dred[warp][1] = neg; S.dred[warp][2] = viol; S.dred[warp][3] = nonfinite;
+        S.dred[warp][4] = bcnt;
+        S.radii[warp] = dmax;  // scratch for the block max
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double Sd = 0, Sda = 0, Sa = 0, Bm = INFINITY, Dm = 0.0, C = 0, NG = 0, VI = 0, NF = 0, BC = 0;
+        for (int q = 0; q < nwarps; ++q) {
+            Sd += S.red[q][0]; Sda += S.red[q][1]; Sa += S.red[q][2]; Bm = fmin(Bm, S.red[q][3]);
+            Dm = fmax(Dm, S.radii[q]);
+            C += S.dred[q][0]; NG += S.dred[q][1]; VI += S.dred[q][2]; NF += S.dred[q][3]; BC += S.dred[q][4];
+        }
+        o[0] = C > 0 ? Sd / C : nan;
+        o[1] = (C > 0 && isfinite(Sa) && Sa > 0.0) ? Sda / Sa : nan;
+        o[2] = a.n_boundary > 0 ? (BC > 0 ? Bm : nan) : INFINITY;
+        const double negf = NF > 0 ? nan : NG / (double)a.n;
+        const double violf = NF > 0 ? nan : VI / (double)a.n;
+        o[3] = negf;
+        o[4] = violf;
+        S.bad = (NF > 0 || negf > 1e-3 || violf > 1e-3) ? 1 : 0;
+        o[5] = S.bad ? 1.0 : 0.0;
+        S.dglob = Dm;
+        const double nb = Dm / w;
+        S.nbins = nb < (double)(kMaxBins - 2) ? (int)nb + 2 : kMaxBins + 1;
+        S.total = a.total_area;
+        S.n_eval = 0;
+        S.rc = a.near_bins;
+    }
+    __syncthreads();
     // A flagged field gets no geometry (core_analysis.py:1558-1564).
-    if (o[5] != 0.0) {
+    if (S.bad || S.nbins > kMaxBins) {
+        if (!S.bad && tid == 0) atomicOr(a.err, KERR_HIST_OVERFLOW);
         for (int i = tid; i < 2 * nt + 2 * ne; i += bs) o[7 + i] = nan;
         if (tid == 0) o[6] = 0.0;
         return;
     }
-    for (int i = tid; i < kMaxBins; i += bs) { S.pre[i] = 0.0; S.ptr[i] = 0; S.fill[i] = 0; }
-    if (tid == 0) { S.nlong = 0; S.n_eval = 0; S.bad_scan = 0; }
-    __syncthreads();
-
-    // pass 1: per-face max distance -> bin histogram, long faces, global max (lean_geometry.py:125-164)
-    const double w = a.width;
-    double tmax = 0.0;
-    for (int f = tid; f < a.nf; f += bs) {
-        const double d0 = (double)d[a.fv[3 * f]], d1 = (double)d[a.fv[3 * f + 1]], d2 = (double)d[a.fv[3 * f + 2]];
-        if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
-        double lo = d0, hi = d0;
-        if (d1 < lo) lo = d1;
-        if (d1 > hi) hi = d1;
-        if (d2 < lo) lo = d2;
-        if (d2 > hi) hi = d2;
-        if (hi - lo > w) {
-            const int idx = atomicAdd(&S.nlong, 1);
-            longf[idx] = f;
-        }
-        if (hi > tmax) tmax = hi;
-        int kb = (int)(hi / w);
-        if (kb < 0) kb = 0;
-        if (kb < kMaxBins) {
-            atomicAdd(&S.pre[kb], a.farea[f]);
-            atomicAdd(&S.ptr[kb], 1);
-        } else {
-            S.bad_scan = 1;
-        }
-    }
-    for (int o2 = 16; o2 > 0; o2 >>= 1) tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o2));
-    if (lane == 0) S.red[warp] = tmax;
-    __syncthreads();
-    if (tid == 0) {
-        double g = 0.0;
-        for (int i = 0; i < nwarps; ++i) g = fmax(g, S.red[i]);
-        const double nb = g / w;
-        S.nbins = nb < (double)(kMaxBins - 2) ? (int)nb + 2 : kMaxBins + 1;
-    }
-    __syncthreads();
-    if (S.nbins > kMaxBins || S.bad_scan) {
-        if (tid == 0) atomicOr(a.err, KERR_HIST_OVERFLOW);
-        for (int i = tid; i < 2 * nt + 2 * ne; i += bs) o[7 + i] = nan;
-        return;
-    }
-    // exclusive prefix sums over bins (warp 0: each lane scans a chunk)
     const int nbins = S.nbins;
-    if (warp == 0) {
-        const int chunk = (nbins + 31) / 32;
-        const int b0 = min(lane * chunk, nbins), b1 = min(b0 + chunk, nbins);
-        double sa = 0.0;
-        int sc = 0;
-        for (int b = b0; b < b1; ++b) { sa += S.pre[b]; sc += S.ptr[b]; }
-        double ea = sa;
-        int ec = sc;
-        for (int o2 = 1; o2 < 32; o2 <<= 1) {
-            const double ta = __shfl_up_sync(0xffffffffu, ea, o2);
-            const int tc = __shfl_up_sync(0xffffffffu, ec, o2);
-            if (lane >= o2) { ea += ta; ec += tc; }
-        }
-        double ra = ea - sa;  // exclusive
-        int rc = ec - sc;
-        for (int b = b0; b < b1; ++b) {
-            const double xa = S.pre[b];
-            const int xc = S.ptr[b];
-            S.pre[b] = ra;
-            S.ptr[b] = rc;
-            ra += xa;
-            rc += xc;
-        }
-        if (lane == 31) { S.total = ea; S.ntot = ec; }
-    }
-    __syncthreads();
+    double tmax = 0.0;
+    for (int t = 0; t < nt; ++t)
+        if (a.targets[t] > tmax && a.targets[t] <= S.total * (1.0 + 1e-12)) tmax = a.targets[t];
 
+    // 2. near faces, with a growing cut if the margin was not enough
     Field<T> F{d, &a, &S, band, longf};
-    // bracket bins of every target -> compacted band range
-    if (tid == 0) {
-        int lo_min = 1 << 30, lo_max = -1;
-        for (int t = 0; t < nt; ++t) {
-            const double target = a.targets[t];
-            if (!(target > 0.0) || target > S.total * (1.0 + 1e-12)) continue;
-            int lo_i = 0, hi_i = nbins;
-            while (lo_i < hi_i) {
-                const int mid = (lo_i + hi_i) / 2;
-                if (F.prefix_at(mid) >= target) hi_i = mid; else lo_i = mid + 1;
+    for (int attempt = 0; attempt < 32; ++attempt) {
+        const int rc = S.rc;
+        for (int i = tid; i <= kMaxBins; i += bs) {
+            S.pre[i] = 0.0;
+            S.ptr[i] = 0;
+            if (i < kMaxBins) S.fill[i] = 0;
+        }
+        if (tid == 0) { S.nlong = 0; S.overflow = 0; }
+        __syncthreads();
+        const double R = rc >= nbins ? INFINITY : rc * w;
+        // vertices closer than R: the shift kernel's near list when R is its radius
+        const bool listed = rc == a.near_bins && rc < nbins;
+        const int nv_scan = listed ? a.near_count[k] : a.n;
+        const int32_t* nl = a.near_list + (int64_t)k * a.n;
+        for (int pass = 0; pass < 2; ++pass) {  // 0: histogram + long faces, 1: counting sort
+            for (int ii = tid; ii < nv_scan; ii += bs) {
+                const int i = listed ? nl[ii] : ii;
+                const double di = (double)d[i];
+                if (!(di < R)) continue;
+                for (int q = a.inc_ptr[i]; q < a.inc_ptr[i + 1]; ++q) {
+                    const int f = a.inc_face[q];
+                    const int c = a.inc_corner[q];
+                    const int v0 = a.fv[3 * f], v1 = a.fv[3 * f + 1], v2 = a.fv[3 * f + 2];
+                    const double d0 = (double)d[v0], d1 = (double)d[v1], d2 = (double)d[v2];
+                    if (c >= 1 && d0 < R) continue;   // an earlier corner emits it
+                    if (c == 2 && d1 < R) continue;
+                    if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
+                    double lo = d0, hi = d0;
+                    if (d1 < lo) lo = d1;
+                    if (d1 > hi) hi = d1;
+                    if (d2 < lo) lo = d2;
+                    if (d2 > hi) hi = d2;
+                    const int kb = F.bin_of(hi);
+                    if (pass == 0) {
+                        if (hi - lo > w) longf[atomicAdd(&S.nlong, 1)] = f;
+                        if (kb <= rc && kb < kMaxBins) {
+                            atomicAdd(&S.pre[kb], a.farea[f]);
+                            atomicAdd(&S.ptr[kb], 1);
+                        }
+                    } else if (kb <= rc && kb < kMaxBins) {
+                        band[S.ptr[kb] + atomicAdd(&S.fill[kb], 1)] = f;
+                    }
+                }
             }
-            lo_min = min(lo_min, lo_i);
-            lo_max = max(lo_max, lo_i);
+            __syncthreads();
+            if (pass == 0) {
+                // exclusive prefix sums over bins [0, min(rc, nbins-1)] by warp 0
+                if (warp == 0) {
+                    const int nbb = min(rc + 1, nbins);
+                    const int chunk = (nbb + 31) / 32;
+                    const int b0 = min(lane * chunk, nbb), b1 = min(b0 + chunk, nbb);
+                    double sa = 0.0;
+                    int sc = 0;
+                    for (int b = b0; b < b1; ++b) { sa += S.pre[b]; sc += S.ptr[b]; }
+                    double ea = sa;
+                    int ec = sc;
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const double ta = __shfl_up_sync(0xffffffffu, ea, off);
+                        const int tc = __shfl_up_sync(0xffffffffu, ec, off);
+                        if (lane >= off) { ea += ta; ec += tc; }
+                    }
+                    double ra = ea - sa;
+                    int rcn = ec - sc;
+                    for (int b = b0; b < b1; ++b) {
+                        const double xa = S.pre[b];
+                        const int xc = S.ptr[b];
+                        S.pre[b] = ra;
+                        S.ptr[b] = rcn;
+                        ra += xa;
+                        rcn += xc;
+                    }
+                    if (lane == 31) {
+                        S.ntot = ec;
+                        S.pre[nbb] = ea;
+                        S.ptr[nbb] = ec;
+                    }
+                }
+                __syncthreads();
+            }
         }
-        if (lo_max < 0) { S.b_lo = 1; S.b_hi = 0; }
-        else { S.b_lo = max(0, lo_min - 2); S.b_hi = min(nbins - 1, lo_max + 1); }
-        S.base = S.b_lo <= S.b_hi ? S.ptr[S.b_lo] : 0;
+        // enough? the largest target must be enclosed two bins below the cut
+        bool ok = rc >= nbins || (rc >= 2 && S.pre[rc - 2] >= tmax);
+        if (ok) break;
+        __syncthreads();
+        if (tid == 0) S.rc = min(nbins, 2 * rc + 4);
+        __syncthreads();
     }
-    __syncthreads();
-    // pass 2: counting sort of the faces of bins [b_lo, b_hi] (lean_geometry.py:168-179)
-    if (S.b_lo <= S.b_hi) {
-        for (int f = tid; f < a.nf; f += bs) {
-            const double d0 = (double)d[a.fv[3 * f]], d1 = (double)d[a.fv[3 * f + 1]], d2 = (double)d[a.fv[3 * f + 2]];
-            if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
-            const int kb = F.bin_of(fmax(fmax(d0, d1), d2));
-            if (kb < S.b_lo || kb > S.b_hi) continue;
-            const int slot = S.ptr[kb] - S.base + atomicAdd(&S.fill[kb], 1);
-            band[slot] = f;
-        }
+    if (S.rc >= nbins) {
+        // every bin is complete: the prefix array covers [0, nbins]
+        if (tid == 0) S.rc = nbins;
     }
     __syncthreads();
 
-    // radii + perimeters, one warp per target (lean_geometry.py:315-324)
+    // 3. radii + perimeters, one warp per target (lean_geometry.py:315-324)
     for (int t = warp; t < nt; t += nwarps) {
         int ev = 0;
         const double r = F.solve_radius(a.targets[t], ev);
@@ -484,25 +584,26 @@ void launch_permute_rows(int32_t n, int32_t cols, const double* in, int32_t in_l
     k_permute_rows<<<blocks, 256, 0, st>>>(n, cols, in, in_ld, in_idx, out, out_ld, out_idx);
 }
 
-template <typename T>
-void launch_vertex_stats(const MetricArgs& a, const T* dT, cudaStream_t st) {
-    if (a.nsrc <= 0) return;
-    k_vertex_stats<T><<<a.nsrc, 256, 0, st>>>(a, dT);
+template <typename Tin, typename Tout>
+void launch_shift_stats(const MetricArgs& a, int32_t K, const Tin* phi, Tout* dT, cudaStream_t st) {
+    if (a.n <= 0 || K <= 0) return;
+    cudaMemsetAsync(a.near_count, 0, (size_t)K * sizeof(int), st);
+    k_shift_stats<Tin, Tout><<<dim3(a.ntiles, K / 32), dim3(32, 8), 0, st>>>(a, K, phi, dT);
 }
 
 template <typename T>
-void launch_geometry(const MetricArgs& a, const T* dT, cudaStream_t st) {
+void launch_source_metrics(const MetricArgs& a, const T* dT, cudaStream_t st) {
     if (a.nsrc <= 0) return;
-    k_geometry<T><<<a.nsrc, 512, 0, st>>>(a, dT);
+    k_source_metrics<T><<<a.nsrc, 512, 0, st>>>(a, dT);
 }
 
 template void launch_shift_transpose<double, double>(int32_t, int32_t, const double*, const int32_t*, double*,
                                                      cudaStream_t);
 template void launch_shift_transpose<float, float>(int32_t, int32_t, const float*, const int32_t*, float*,
                                                    cudaStream_t);
-template void launch_vertex_stats<double>(const MetricArgs&, const double*, cudaStream_t);
-template void launch_vertex_stats<float>(const MetricArgs&, const float*, cudaStream_t);
-template void launch_geometry<double>(const MetricArgs&, const double*, cudaStream_t);
-template void launch_geometry<float>(const MetricArgs&, const float*, cudaStream_t);
+template void launch_shift_stats<double, double>(const MetricArgs&, int32_t, const double*, double*, cudaStream_t);
+template void launch_shift_stats<float, float>(const MetricArgs&, int32_t, const float*, float*, cudaStream_t);
+template void launch_source_metrics<double>(const MetricArgs&, const double*, cudaStream_t);
+template void launch_source_metrics<float>(const MetricArgs&, const float*, cudaStream_t);
 
 }  // namespace fcw

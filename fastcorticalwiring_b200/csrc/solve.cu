@@ -38,6 +38,7 @@ constexpr int KT = kRhsTile;    // right-hand sides per CTA
 constexpr int LDS = KT + 1;
 constexpr int LDP = TR + 1;
 constexpr int RC = 32;          // structure rows per staged chunk in the backward gather
+constexpr int kGatherStage = 1024;  // gather entries staged in shared memory per forward task
 
 template <typename T>
 __device__ __forceinline__ void zero(T (&acc)[4][4]) {
@@ -81,12 +82,47 @@ __device__ __forceinline__ void mma_cols(T (&acc)[4][4], const T* A, int lda, co
     }
 }
 
+// rows [f0, f0+nf) of supernode s's front (fb = its first front row): out[r][c] =
+// init(r, k) + sign * sum of the children's update rows listed for front row f0+r,
+// for this CTA's 64 columns. Entries are staged in shared memory when they fit;
+// each thread owns one column and every 4th row, so its loads are independent.
+template <typename T, typename Init>
+__device__ __forceinline__ void gather_rows(const SolveArgs<T>& a, int64_t fb, int f0, int nrows, T* out, Init init,
+                                            T sign, int* gsrc, int* gchild, int* grs) {
+    const int tid = threadIdx.x;
+    const int K = a.K, k0 = blockIdx.y * KT;
+    const int eb = a.gm_ptr[fb + f0];
+    const int E = a.gm_ptr[fb + f0 + nrows] - eb;
+    const bool staged = E <= kGatherStage;
+    for (int r = tid; r <= nrows; r += 256) grs[r] = a.gm_ptr[fb + f0 + r] - eb;
+    if (staged)
+        for (int e = tid; e < E; e += 256) {
+            gsrc[e] = a.gm_src[eb + e];
+            gchild[e] = a.gm_child[eb + e];
+        }
+    __syncthreads();
+    const int c = tid & (KT - 1), k = k0 + c;
+    for (int r = tid / KT; r < nrows; r += 256 / KT) {
+        T v = init(r, k);
+        const int e0 = grs[r], e1 = grs[r + 1];
+        for (int e = e0; e < e1; ++e) {
+            const int src = staged ? gsrc[e] : a.gm_src[eb + e];
+            const int ch = staged ? gchild[e] : a.gm_child[eb + e];
+            if (a.reach && !a.reach[ch]) continue;
+            v += sign * a.U[(int64_t)src * K + k];
+        }
+        out[r * LDS + c] = v;
+    }
+    __syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_fwd(SolveArgs<T> a, int32_t t0) {
     extern __shared__ __align__(16) unsigned char smraw[];
     T* Ws = reinterpret_cast<T*>(smraw);   // TR x LDS
     T* Xs = Ws + TR * LDS;                  // TR x LDS
     T* Ms = Xs + TR * LDS;                  // TR x LDP
+    __shared__ int gsrc[kGatherStage], gchild[kGatherStage], grs[TR + 1];
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, chunk = task.y;
     if (a.reach && !a.reach[s]) return;
@@ -97,22 +133,13 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs<T> a, int32_t t0) {
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, m = p.sn_m[s], nr = m - ns;
     const int64_t fb = p.sn_rowptr[s];
 
-    // W = right-hand side of s's columns minus the children's updates on them
-    for (int f = warp; f < ns; f += 8) {
-        const int e0 = a.gm_ptr[fb + f], e1 = a.gm_ptr[fb + f + 1];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int c = lane + 32 * h, k = k0 + c;
-            T v;
-            if (a.delta_src) v = (a.delta_src[k] == c0 + f) ? T(1) : T(0);
-            else v = a.R[(int64_t)(c0 + f) * K + k];
-            for (int e = e0; e < e1; ++e) {
-                if (a.reach && !a.reach[a.gm_child[e]]) continue;
-                v -= a.U[(int64_t)a.gm_src[e] * K + k];
-            }
-            Ws[f * LDS + c] = v;
-        }
-    }
+    // W = right-hand side of s's columns minus the children's updates on them.
+    // The gather entries of these rows are contiguous; stage them in shared memory
+    // so every (row, column) accumulation issues independent, coalesced loads.
+    gather_rows<T>(a, fb, 0, ns, Ws, [&](int f, int k) -> T {
+        if (a.delta_src) return (a.delta_src[k] == c0 + f) ? T(1) : T(0);
+        return a.R[(int64_t)(c0 + f) * K + k];
+    }, T(-1), gsrc, gchild, grs);
     const T* inv = a.inv + p.sn_invptr[s];
     for (int e = tid; e < ns * ns; e += 256) {
         const int i = e / ns, j = e - i * ns;
@@ -155,20 +182,13 @@ __global__ void __launch_bounds__(256) k_fwd(SolveArgs<T> a, int32_t t0) {
             for (int b = 0; b < 4; ++b) Ws[r * LDS + tx + 16 * b] = acc[aa][b];
     }
     __syncthreads();
+    // U_s rows of this chunk = L_rs X_s (in Ws) + the children's updates landing on them
+    gather_rows<T>(a, fb, ns + q0, nq, Ws, [&](int r, int k) -> T { return Ws[r * LDS + (k - k0)]; }, T(1), gsrc,
+                   gchild, grs);
     T* Us = a.U + (a.uoff[s] + q0) * (int64_t)K;
-    for (int r = warp; r < nq; r += 8) {
-        const int f = ns + q0 + r;
-        const int e0 = a.gm_ptr[fb + f], e1 = a.gm_ptr[fb + f + 1];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int c = lane + 32 * h, k = k0 + c;
-            T v = Ws[r * LDS + c];
-            for (int e = e0; e < e1; ++e) {
-                if (a.reach && !a.reach[a.gm_child[e]]) continue;
-                v += a.U[(int64_t)a.gm_src[e] * K + k];
-            }
-            Us[(int64_t)r * K + k] = v;
-        }
+    for (int e = tid; e < nq * KT; e += 256) {
+        const int r = e / KT, c = e - r * KT;
+        Us[(int64_t)r * K + k0 + c] = Ws[r * LDS + c];
     }
 }
 
@@ -178,7 +198,7 @@ __global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
     T* Ps = reinterpret_cast<T*>(smraw);   // RC x LDP  panel rows of the chunk
     T* Xg = Ps + RC * LDP;                  // RC x LDS  gathered solution rows
     T* Cs = Xg + RC * LDS;                  // TR x LDS
-    T* Ms = Cs + TR * LDS;                  // TR x LDP  inverse diagonal block
+    T* Ms = Ps;                             // TR x LDP  inverse diagonal block, after the gather
     __shared__ int last_arrival;
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, split = task.y;
@@ -288,7 +308,8 @@ __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __res
 template <typename T>
 constexpr size_t fwd_smem() { return (size_t)(2 * TR * LDS + TR * LDP) * sizeof(T); }
 template <typename T>
-constexpr size_t bwd_smem() { return (size_t)(RC * LDP + RC * LDS + TR * LDS + TR * LDP) * sizeof(T); }
+constexpr size_t bwd_smem() { return (size_t)(RC * LDP + RC * LDS + TR * LDS) * sizeof(T); }
+static_assert(RC * LDP + RC * LDS >= TR * LDP, "the inverse tile aliases the gather staging area");
 
 }  // namespace
 

@@ -86,12 +86,11 @@ enum {
     FCW_STAGE_POISSON_FWD = 3,
     FCW_STAGE_POISSON_BWD = 4,
     FCW_STAGE_SHIFT = 5,         /* phi -= phi[source], transpose to one field per source */
-    FCW_STAGE_VERTEX_STATS = 6,  /* health screen, MSD, distance to boundary */
-    FCW_STAGE_GEOMETRY = 7,      /* radius inversion, perimeter, samples */
-    FCW_N_STAGES = 8
+    FCW_STAGE_METRICS = 6,       /* health, MSD, distance to boundary, radius inversion, perimeter, samples */
+    FCW_N_STAGES = 7
 };
 
-/* Fill *p with the defaults (0.7 mm, 1e-10, K=256, leaf 64, width 64, relax 32, mixed on). */
+/* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 32, mixed on). */
 void fcw_default_params(fcw_params* p);
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between);
