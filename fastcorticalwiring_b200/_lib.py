@@ -25,7 +25,7 @@ EXPORTED = (
     "fcw_engine_create", "fcw_engine_info", "fcw_engine_destroy", "fcw_compute_distance",
     "fcw_compute_distances", "fcw_compute_metrics", "fcw_compute_metrics_device", "fcw_synchronize",
     "fcw_heat_solve_device", "fcw_divergence_device", "fcw_poisson_solve_device", "fcw_field_metrics_device",
-    "fcw_engine_profile", "fcw_engine_stage_times",
+    "fcw_engine_profile", "fcw_engine_stage_times", "fcw_field_metrics_static",
 )
 STAGES = ("heat_fwd", "heat_bwd", "divergence", "poisson_fwd", "poisson_bwd", "shift", "metrics")
 
@@ -101,6 +101,7 @@ def load():
         "fcw_divergence_device": (ctypes.c_int, [P, P, I32, P, P]),
         "fcw_poisson_solve_device": (ctypes.c_int, [P, P, P, I32, P, P]),
         "fcw_field_metrics_device": (ctypes.c_int, [P, P, P, I32, P, I32, I32, D, P, P]),
+        "fcw_field_metrics_static": (ctypes.c_int, [P, P, P, I32, P, I32, I32, D, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

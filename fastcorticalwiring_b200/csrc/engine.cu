@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1033,3 +1034,105 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free field metrics
+//
+// For callers that may not allocate device memory once they are running: a host
+// that reserves the whole device up front for its own pool, or a measurement or
+// serving loop that must keep its device footprint fixed. This entry point runs
+// the same kernels as fcw_field_metrics_device, but every buffer it needs beyond
+// the caller's inputs and outputs (and the engine's own arrays, allocated when
+// the engine was created) comes from one fixed array compiled into the library.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Per-call scratch for fcw_field_metrics_static. Every device that loads this
+// library holds these bytes until the process exits.
+constexpr size_t kStaticScratchBytes = 64u << 20;
+constexpr int32_t kStaticMaxFields = 32;
+static __device__ __align__(256) unsigned char g_field_scratch[kStaticScratchBytes];
+
+// The array's device address, looked up once per device. In host code the name
+// g_field_scratch only stands in for the symbol; it is not a device pointer.
+constexpr int kMaxDevices = 64;
+void* g_field_scratch_addr[kMaxDevices] = {nullptr};
+std::mutex g_field_scratch_mutex;
+
+int static_scratch_address(int device, unsigned char** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(FCW_E_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_field_scratch_mutex);
+    if (!g_field_scratch_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&p, g_field_scratch);  // the engine's device is current
+        if (rc != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            return fail(FCW_E_CUDA, std::string("cudaGetSymbolAddress(static field scratch) failed: ") +
+                                        cudaGetErrorString(rc));
+        }
+        g_field_scratch_addr[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_field_scratch_addr[device]);
+    return FCW_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" int fcw_field_metrics_static(fcw_engine* e, const double* d_dev, const int32_t* sources_dev, int32_t k,
+                                        const double* targets, int32_t nt, int32_t nb, double eps, double* out_dev,
+                                        void* stream) {
+    FCW_TRY(check_engine(e));
+    if (k <= 0 || !d_dev || !sources_dev || !out_dev) return fail(FCW_E_INVALID, "invalid arguments");
+    if (k > kStaticMaxFields)
+        return fail(FCW_E_INVALID, "fcw_field_metrics_static takes at most " + std::to_string(kStaticMaxFields) +
+                                       " fields per call, got " + std::to_string(k));
+    const int32_t K = 32;  // one 32-column tile of the shift kernel; columns >= k are padding
+    const int64_t n = e->sym.n, nf = e->mesh.nf;
+    const int64_t ntiles = (n + fcw::kStatVTile - 1) / fcw::kStatVTile;
+    const size_t need = align256((size_t)n * K * sizeof(double))          // vertex-major fields
+                        + align256((size_t)n * K * sizeof(double))        // shifted, one field per row
+                        + align256((size_t)ntiles * K * 8 * sizeof(double))  // health/MSD partials
+                        + align256((size_t)n * K * sizeof(int32_t))       // near-vertex lists
+                        + align256((size_t)K * sizeof(int32_t))           // near-vertex counts
+                        + 2 * align256((size_t)nf * K * sizeof(int32_t))  // near faces by bin, long faces
+                        + align256((size_t)K * sizeof(int32_t));          // sources (elimination order)
+    if (need > kStaticScratchBytes)
+        return fail(FCW_E_INVALID, "mesh too large for fcw_field_metrics_static: needs " + std::to_string(need) +
+                                       " bytes of scratch, the static array holds " +
+                                       std::to_string(kStaticScratchBytes));
+    unsigned char* base = nullptr;
+    FCW_TRY(static_scratch_address(e->device, &base));
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base + off;
+        off += align256(bytes);
+        return p;
+    };
+    double* Y = reinterpret_cast<double*>(take((size_t)n * K * sizeof(double)));
+    double* dT = reinterpret_cast<double*>(take((size_t)n * K * sizeof(double)));
+    double* partials = reinterpret_cast<double*>(take((size_t)ntiles * K * 8 * sizeof(double)));
+    int32_t* near_list = reinterpret_cast<int32_t*>(take((size_t)n * K * sizeof(int32_t)));
+    int32_t* near_count = reinterpret_cast<int32_t*>(take((size_t)K * sizeof(int32_t)));
+    int32_t* band = reinterpret_cast<int32_t*>(take((size_t)nf * K * sizeof(int32_t)));
+    int32_t* longf = reinterpret_cast<int32_t*>(take((size_t)nf * K * sizeof(int32_t)));
+    int32_t* src = reinterpret_cast<int32_t*>(take((size_t)K * sizeof(int32_t)));
+
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    fcw::MetricArgs a;
+    FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
+    a.src = src;
+    a.band = band;
+    a.longf = longf;
+    a.partials = partials;
+    a.near_list = near_list;
+    a.near_count = near_count;  // cleared by launch_shift_stats before the shift kernel
+    a.out = out_dev;
+    k_map_sources<<<1, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)n, K, src, e->err_d);
+    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)n, k, K, d_dev, e->iperm_d, Y);
+    fcw::launch_shift_stats<double, double>(a, K, Y, dT, st);
+    fcw::launch_source_metrics<double>(a, dT, st);
+    FCW_CUDA(cudaGetLastError());
+    return FCW_OK;
+}

@@ -171,6 +171,21 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
                              const double* targets_host, int32_t n_targets, int32_t n_between, double eps,
                              double* out_dev, void* stream);
 
+/* Allocation-free field metrics, for callers that may not allocate device
+ * memory while they run: a host that reserves the device for its own memory
+ * pool, or a loop that must keep its device footprint fixed. Same arguments and
+ * results as fcw_field_metrics_device; this entry point has no counterpart in
+ * the reference. Its scratch is one 64 MiB array compiled into the library
+ * (held by every device that loads it until the process exits); it takes at most
+ * 32 fields per call and rejects meshes whose scratch would not fit with
+ * FCW_E_INVALID (roughly 40k vertices with 32 fields). It calls no allocator.
+ * The first call on each device looks up the array's device address; make that
+ * call before any stream capture. Every call reuses the same array, so calls
+ * that overlap on the GPU (other streams, other threads) race: serialise them. */
+int fcw_field_metrics_static(fcw_engine* e, const double* d_dev, const int32_t* sources_dev, int32_t k,
+                             const double* targets_host, int32_t n_targets, int32_t n_between, double eps,
+                             double* out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
