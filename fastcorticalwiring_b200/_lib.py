@@ -40,7 +40,7 @@ class FCWParams(ctypes.Structure):
         ("relax", ctypes.c_int32),
         ("build_mixed", ctypes.c_int32),
         ("device", ctypes.c_int32),
-        ("refine_steps", ctypes.c_int32),
+        ("pipeline_depth", ctypes.c_int32),
     ]
 
 

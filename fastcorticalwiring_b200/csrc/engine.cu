@@ -88,6 +88,9 @@ struct Workspace {
     double* partials = nullptr; // per (vertex tile, source) health/MSD partial sums
     int32_t* near_list = nullptr;
     int32_t* near_count = nullptr;
+    cudaStream_t stream = nullptr;  // this workspace's stream in the pipelined device path
+    cudaEvent_t done = nullptr;
+    std::vector<std::pair<int, cudaEvent_t>> marks;  // stage timeline on this workspace
     double* part = nullptr;     // backward split-K partial sums
     int* counters = nullptr;    // split-K arrival tickets, zero at rest
 };
@@ -121,12 +124,17 @@ struct fcw_engine {
            *g22_d = nullptr;
     int32_t* boundary_d = nullptr;
     int* err_d = nullptr;
-    Workspace ws;
+    std::vector<Workspace> pool;  // blocks in flight: workspace i runs on pool[i].stream
+    size_t cur_ws = 0;
+    Workspace& cw() { return pool[cur_ws]; }
+    cudaEvent_t ev_in = nullptr;  // the caller's stream at the start of a pipelined call
+    int32_t* hsrc_d = nullptr;    // staging for the host-buffer metrics API
+    double* hout_d = nullptr;
+    int64_t hcap_src = 0, hcap_out = 0;
     double analyze_ms = 0.0, factor_ms = 0.0;
     double lean_total = 0.0;  // sum of the lean face areas (the prefix total of a finite field)
     // stage timeline (CUDA events on the working stream), off unless enabled
     bool prof_on = false;
-    std::vector<std::pair<int, cudaEvent_t>> marks;
     std::vector<cudaEvent_t> event_pool;
     double stage_ms[FCW_N_STAGES] = {0};
     int64_t launches = 0;
@@ -162,7 +170,12 @@ struct fcw_engine {
             }
     }
     ~fcw_engine() {
-        for (auto& m : marks) cudaEventDestroy(m.second);
+        for (auto& w : pool) {
+            for (auto& m : w.marks) cudaEventDestroy(m.second);
+            if (w.done) cudaEventDestroy(w.done);
+            if (w.stream) cudaStreamDestroy(w.stream);
+        }
+        if (ev_in) cudaEventDestroy(ev_in);
         for (cudaEvent_t ev : event_pool) cudaEventDestroy(ev);
         for (void* p : allocs) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
@@ -199,21 +212,24 @@ void mark(fcw_engine* e, cudaStream_t st, int stage) {
         return;
     }
     cudaEventRecord(ev, st);
-    e->marks.push_back({stage, ev});
+    e->cw().marks.push_back({stage, ev});
 }
 
 int collect_marks(fcw_engine* e) {
-    if (e->marks.empty()) return FCW_OK;
-    FCW_CUDA(cudaEventSynchronize(e->marks.back().second));
-    for (size_t j = 0; j + 1 < e->marks.size(); ++j) {
-        const int stg = e->marks[j].first;
-        if (stg < 0 || stg >= FCW_N_STAGES) continue;
-        float ms = 0.0f;
-        FCW_CUDA(cudaEventElapsedTime(&ms, e->marks[j].second, e->marks[j + 1].second));
-        e->stage_ms[stg] += ms;
+    for (auto& w : e->pool) {
+        auto& marks = w.marks;
+        if (marks.empty()) continue;
+        FCW_CUDA(cudaEventSynchronize(marks.back().second));
+        for (size_t j = 0; j + 1 < marks.size(); ++j) {
+            const int stg = marks[j].first;
+            if (stg < 0 || stg >= FCW_N_STAGES) continue;
+            float ms = 0.0f;
+            FCW_CUDA(cudaEventElapsedTime(&ms, marks[j].second, marks[j + 1].second));
+            e->stage_ms[stg] += ms;
+        }
+        for (auto& m : marks) e->event_pool.push_back(m.second);
+        marks.clear();
     }
-    for (auto& m : e->marks) e->event_pool.push_back(m.second);
-    e->marks.clear();
     return FCW_OK;
 }
 
@@ -227,7 +243,7 @@ int validate_params(const fcw_params* p) {
     if (p->leaf_size < 1 || p->max_width < 1 || p->max_width > fcw::kMaxWidth)
         return fail(FCW_E_INVALID, "max_width must be in [1, 64] and leaf_size >= 1");
     if (p->relax < 1 || p->relax > p->max_width) return fail(FCW_E_INVALID, "relax must be in [1, max_width]");
-    if (p->refine_steps < 0 || p->refine_steps > 8) return fail(FCW_E_INVALID, "refine_steps must be in [0, 8]");
+    if (p->pipeline_depth < 1 || p->pipeline_depth > 4) return fail(FCW_E_INVALID, "pipeline_depth must be in [1, 4]");
     return FCW_OK;
 }
 
@@ -282,6 +298,12 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     FCW_CUDA(fcw::configure_kernels());
     FCW_CUDA(fcw::configure_solve_kernels());
     FCW_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    FCW_CUDA(cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming));
+    e->pool.resize((size_t)std::max(1, e->prm.pipeline_depth));
+    for (auto& w : e->pool) {
+        FCW_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking));
+        FCW_CUDA(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming));
+    }
     FCW_TRY(e->dalloc(&e->err_d, 1));
     FCW_CUDA(cudaMemset(e->err_d, 0, sizeof(int)));
 
@@ -494,23 +516,26 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     return FCW_OK;
 }
 
-int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
-    Workspace& w = e->ws;
+int ensure_one(fcw_engine* e, Workspace& w, int32_t K, int32_t stride) {
     if (w.K >= K && w.out_stride >= stride) return FCW_OK;
     const int32_t Kn = std::max(K, w.K);
     const int32_t sn = std::max(stride, w.out_stride);
-    void* old[] = {w.Bh, w.Bp64, w.Bp32, w.Y, w.dT64, w.dT32, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
+    void* old[] = {w.Bh, w.Bp64, w.Y, w.dT64, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
                    w.counters, w.partials, w.near_list, w.near_count};
     for (void* p : old)
         if (p) e->release(p);
+    cudaStream_t stream = w.stream;
+    cudaEvent_t done = w.done;
     w = Workspace{};
+    w.stream = stream;
+    w.done = done;
     const int64_t n = e->sym.n, nf = e->mesh.nf;
     FCW_TRY(e->dalloc(&w.Bh, (size_t)n * Kn));
     FCW_TRY(e->dalloc(&w.Bp64, (size_t)n * Kn));
-    FCW_TRY(e->dalloc(&w.Bp32, (size_t)n * Kn));
+    w.Bp32 = reinterpret_cast<float*>(w.Bp64);  // a block uses one precision
     FCW_TRY(e->dalloc(&w.Y, (size_t)n * Kn));
     FCW_TRY(e->dalloc(&w.dT64, (size_t)n * Kn));
-    FCW_TRY(e->dalloc(&w.dT32, (size_t)n * Kn));
+    w.dT32 = reinterpret_cast<float*>(w.dT64);
     FCW_TRY(e->dalloc(&w.src, (size_t)Kn));
     FCW_TRY(e->dalloc(&w.reach, (size_t)std::max<int64_t>(e->sym.nsuper, 1)));
     FCW_TRY(e->dalloc(&w.band, (size_t)nf * Kn));
@@ -530,6 +555,12 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
     return FCW_OK;
 }
 
+// Every workspace of the pool holds at least K columns and `stride` output doubles per column.
+int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
+    for (auto& w : e->pool) FCW_TRY(ensure_one(e, w, K, stride));
+    return FCW_OK;
+}
+
 template <typename T>
 fcw::SolveArgs<T> solve_args(fcw_engine* e, const T* val, const T* inv, T* B, int32_t K) {
     fcw::SolveArgs<T> a;
@@ -538,16 +569,16 @@ fcw::SolveArgs<T> solve_args(fcw_engine* e, const T* val, const T* inv, T* B, in
     a.inv = inv;
     a.B = B;
     a.K = K;
-    a.U = reinterpret_cast<T*>(e->ws.U);
+    a.U = reinterpret_cast<T*>(e->cw().U);
     a.uoff = e->uoff_d;
     a.gm_ptr = e->gm_ptr_d;
     a.gm_src = e->gm_src_d;
     a.gm_child = e->gm_child_d;
     a.nsplit = e->nsplit_d;
     a.poff = e->poff_d;
-    a.part = reinterpret_cast<T*>(e->ws.part);
-    a.counters = e->ws.counters;
-    a.ktiles = e->ws.K / fcw::kRhsTile;
+    a.part = reinterpret_cast<T*>(e->cw().part);
+    a.counters = e->cw().counters;
+    a.ktiles = e->cw().K / fcw::kRhsTile;
     return a;
 }
 
@@ -570,7 +601,7 @@ void sweep(fcw_engine* e, fcw::SolveArgs<T> a, cudaStream_t st, int stage_fwd, i
 
 // Heat solve for the K sources in ws.src: u (elimination order, n x K) in ws.Bh.
 void heat_solve(fcw_engine* e, int32_t K, cudaStream_t st) {
-    Workspace& w = e->ws;
+    Workspace& w = e->cw();
     mark(e, st, FCW_STAGE_HEAT_FWD);
     fcw::launch_reach(e->plan, w.src, K, w.reach, st);
     e->launches += 2;
@@ -591,7 +622,7 @@ void poisson_solve(fcw_engine* e, const T* val, const T* inv, const T* R, T* Y, 
 // Distances for the K sources in ws.src, shifted, source-major in ws.dT64 / ws.dT32.
 // With metric arguments, the shift also produces the health/MSD partials and near lists.
 void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, const fcw::MetricArgs* ma = nullptr) {
-    Workspace& w = e->ws;
+    Workspace& w = e->cw();
     const int32_t n = (int32_t)e->sym.n;
     heat_solve(e, K, st);
     mark(e, st, FCW_STAGE_DIVERGENCE);
@@ -648,9 +679,9 @@ int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, do
     for (int32_t j = 0; j < nb; ++j) a.fracs[j] = (double)(j + 1) / ((double)nb + 1.0);
     a.K = nsrc;
     a.ntiles = (int32_t)((e->sym.n + fcw::kStatVTile - 1) / fcw::kStatVTile);
-    a.partials = e->ws.partials;
-    a.near_list = e->ws.near_list;
-    a.near_count = e->ws.near_count;
+    a.partials = e->cw().partials;
+    a.near_list = e->cw().near_list;
+    a.near_count = e->cw().near_count;
     {
         // near radius: a flat disc holding twice the largest reachable target, in whole bins
         double tmax = 0.0;
@@ -660,10 +691,10 @@ int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, do
         a.near_bins = (int32_t)std::ceil(r0 / e->mesh.bin_width) + 2;
         a.near_radius = (double)a.near_bins * e->mesh.bin_width;
     }
-    a.src = e->ws.src;
-    a.band = e->ws.band;
-    a.longf = e->ws.longf;
-    a.out = e->ws.out;
+    a.src = e->cw().src;
+    a.band = e->cw().band;
+    a.longf = e->cw().longf;
+    a.out = e->cw().out;
     a.err = e->err_d;
     return FCW_OK;
 }
@@ -693,7 +724,7 @@ int map_sources_host(fcw_engine* e, const int32_t* sources, int64_t n, int32_t K
                                            std::to_string(e->sym.n) + " vertices");
         buf[k] = e->sym.iperm[s];
     }
-    FCW_CUDA(cudaMemcpyAsync(e->ws.src, buf.data(), K * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    FCW_CUDA(cudaMemcpyAsync(e->cw().src, buf.data(), K * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     return FCW_OK;
 }
 
@@ -716,7 +747,7 @@ void fcw_default_params(fcw_params* p) {
     p->relax = 32;
     p->build_mixed = 1;
     p->device = 0;
-    p->refine_steps = 0;
+    p->pipeline_depth = 2;
 }
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between) {
@@ -860,18 +891,18 @@ int fcw_compute_distances(fcw_engine* e, const int32_t* sources, int64_t n, int3
     for (int64_t b0 = 0; b0 < n; b0 += Kmax) {
         const int64_t nb = std::min<int64_t>(Kmax, n - b0);
         const int32_t K = round_k(nb);
-        FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
+        FCW_TRY(ensure_workspace(e, K, e->cw().out_stride));
         FCW_TRY(map_sources_host(e, sources + b0, nb, K, e->stream, buf));
         distances_block(e, K, precision, e->stream);
         FCW_CUDA(cudaGetLastError());
         for (int64_t r = 0; r < nb; ++r) {
             if (precision == FCW_PREC_MIXED) {
-                FCW_CUDA(cudaMemcpyAsync(rowbuf32.data(), e->ws.dT32 + r * nv, nv * sizeof(float),
+                FCW_CUDA(cudaMemcpyAsync(rowbuf32.data(), e->cw().dT32 + r * nv, nv * sizeof(float),
                                          cudaMemcpyDeviceToHost, e->stream));
                 FCW_CUDA(cudaStreamSynchronize(e->stream));
                 for (int64_t i = 0; i < nv; ++i) out_host[(b0 + r) * nv + i] = (double)rowbuf32[e->sym.iperm[i]];
             } else {
-                FCW_CUDA(cudaMemcpyAsync(rowbuf.data(), e->ws.dT64 + r * nv, nv * sizeof(double),
+                FCW_CUDA(cudaMemcpyAsync(rowbuf.data(), e->cw().dT64 + r * nv, nv * sizeof(double),
                                          cudaMemcpyDeviceToHost, e->stream));
                 FCW_CUDA(cudaStreamSynchronize(e->stream));
                 for (int64_t i = 0; i < nv; ++i) out_host[(b0 + r) * nv + i] = rowbuf[e->sym.iperm[i]];
@@ -886,57 +917,80 @@ int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host) {
     return fcw_compute_distances(e, &source, 1, FCW_PREC_FP64, out_host);
 }
 
-int fcw_compute_metrics(fcw_engine* e, const int32_t* sources, int64_t n, int32_t precision, const double* targets,
-                        int32_t nt, int32_t nb, double eps, double* out_host) {
-    FCW_TRY(check_engine(e));
-    if (n < 0 || (n > 0 && (!sources || !out_host))) return fail(FCW_E_INVALID, "NULL argument");
-    if (precision == FCW_PREC_MIXED && !e->val_g) return fail(FCW_E_INVALID, "engine was built without the mixed form");
-    const int32_t stride = fcw_metrics_stride(nt, nb);
-    const int32_t Kmax = e->prm.block_k;
-    std::vector<int32_t> buf;
-    for (int64_t b0 = 0; b0 < n; b0 += Kmax) {
-        const int64_t nbk = std::min<int64_t>(Kmax, n - b0);
-        const int32_t K = round_k(nbk);
-        FCW_TRY(ensure_workspace(e, K, stride));
-        fcw::MetricArgs a;
-        FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
-        FCW_TRY(map_sources_host(e, sources + b0, nbk, K, e->stream, buf));
-        distances_block(e, K, precision, e->stream, &a);
-        if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, e->ws.dT32, e->stream);
-        else metrics_block<double>(e, a, e->ws.dT64, e->stream);
-        FCW_CUDA(cudaGetLastError());
-        FCW_CUDA(cudaMemcpyAsync(out_host + b0 * stride, e->ws.out, nbk * stride * sizeof(double),
-                                 cudaMemcpyDeviceToHost, e->stream));
-        FCW_TRY(check_kernel_errors(e, "metrics"));
-    }
-    return FCW_OK;
-}
-
 int fcw_compute_metrics_device(fcw_engine* e, const int32_t* sources_dev, int64_t n, int32_t precision,
                                const double* targets, int32_t nt, int32_t nb, double eps, double* out_dev,
                                void* stream) {
     FCW_TRY(check_engine(e));
     if (n < 0 || (n > 0 && (!sources_dev || !out_dev))) return fail(FCW_E_INVALID, "NULL argument");
     if (precision == FCW_PREC_MIXED && !e->val_g) return fail(FCW_E_INVALID, "engine was built without the mixed form");
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n == 0) return FCW_OK;
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
     const int32_t stride = fcw_metrics_stride(nt, nb);
     const int32_t Kmax = e->prm.block_k;
-    for (int64_t b0 = 0; b0 < n; b0 += Kmax) {
+    FCW_TRY(ensure_workspace(e, std::min<int64_t>(round_k(n), Kmax), stride));
+    // Blocks of K sources round-robin over the workspace pool, each workspace on its own
+    // stream, so independent blocks overlap. The pool streams start after the caller's
+    // stream reaches this call, and the caller's stream waits for all of them at the end.
+    const size_t depth = e->pool.size();
+    FCW_CUDA(cudaEventRecord(e->ev_in, user));
+    size_t used = 0;
+    int rc = FCW_OK;
+    for (int64_t b0 = 0, blk = 0; b0 < n && rc == FCW_OK; b0 += Kmax, ++blk) {
         const int64_t nbk = std::min<int64_t>(Kmax, n - b0);
         const int32_t K = round_k(nbk);
-        FCW_TRY(ensure_workspace(e, K, stride));
+        e->cur_ws = (size_t)blk % depth;
+        Workspace& w = e->cw();
+        if (blk < (int64_t)depth) {
+            FCW_CUDA(cudaStreamWaitEvent(w.stream, e->ev_in, 0));
+            used = (size_t)blk + 1;
+        }
         fcw::MetricArgs a;
-        FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
+        rc = metric_args(e, targets, nt, nb, eps, K, a);
+        if (rc != FCW_OK) break;
         a.out = out_dev + b0 * stride;
-        k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(nbk, sources_dev + b0, e->iperm_d, (int32_t)e->sym.n, K,
-                                                       e->ws.src, e->err_d);
+        k_map_sources<<<(K + 127) / 128, 128, 0, w.stream>>>(nbk, sources_dev + b0, e->iperm_d, (int32_t)e->sym.n, K,
+                                                             w.src, e->err_d);
         e->launches += 1;
-        distances_block(e, K, precision, st, &a);
-        if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, e->ws.dT32, st);
-        else metrics_block<double>(e, a, e->ws.dT64, st);
-        FCW_CUDA(cudaGetLastError());
+        distances_block(e, K, precision, w.stream, &a);
+        if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, w.dT32, w.stream);
+        else metrics_block<double>(e, a, w.dT64, w.stream);
     }
+    for (size_t i = 0; i < used; ++i) {
+        FCW_CUDA(cudaEventRecord(e->pool[i].done, e->pool[i].stream));
+        FCW_CUDA(cudaStreamWaitEvent(user, e->pool[i].done, 0));
+    }
+    e->cur_ws = 0;
+    if (rc != FCW_OK) return rc;
+    FCW_CUDA(cudaGetLastError());
     return FCW_OK;
+}
+
+int fcw_compute_metrics(fcw_engine* e, const int32_t* sources, int64_t n, int32_t precision, const double* targets,
+                        int32_t nt, int32_t nb, double eps, double* out_host) {
+    FCW_TRY(check_engine(e));
+    if (n < 0 || (n > 0 && (!sources || !out_host))) return fail(FCW_E_INVALID, "NULL argument");
+    if (n == 0) return FCW_OK;
+    for (int64_t k = 0; k < n; ++k)
+        if (sources[k] < 0 || sources[k] >= e->sym.n)
+            return fail(FCW_E_INVALID, "source_idx out of range: " + std::to_string(sources[k]) + " for mesh with " +
+                                           std::to_string(e->sym.n) + " vertices");
+    const int32_t stride = fcw_metrics_stride(nt, nb);
+    if (e->hcap_src < n) {
+        if (e->hsrc_d) e->release(e->hsrc_d);
+        e->hsrc_d = nullptr;
+        FCW_TRY(e->dalloc(&e->hsrc_d, (size_t)n));
+        e->hcap_src = n;
+    }
+    if (e->hcap_out < n * stride) {
+        if (e->hout_d) e->release(e->hout_d);
+        e->hout_d = nullptr;
+        FCW_TRY(e->dalloc(&e->hout_d, (size_t)n * stride));
+        e->hcap_out = n * stride;
+    }
+    FCW_CUDA(cudaMemcpyAsync(e->hsrc_d, sources, n * sizeof(int32_t), cudaMemcpyHostToDevice, e->stream));
+    FCW_TRY(fcw_compute_metrics_device(e, e->hsrc_d, n, precision, targets, nt, nb, eps, e->hout_d, e->stream));
+    FCW_CUDA(cudaMemcpyAsync(out_host, e->hout_d, n * stride * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    return check_kernel_errors(e, "metrics");
 }
 
 int fcw_engine_profile(fcw_engine* e, int enable) {
@@ -967,12 +1021,12 @@ int fcw_heat_solve_device(fcw_engine* e, const int32_t* sources_dev, int32_t k, 
     if (k <= 0 || !sources_dev || !u_dev) return fail(FCW_E_INVALID, "invalid arguments");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int32_t K = round_k(k);
-    FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
-    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->ws.src,
+    FCW_TRY(ensure_workspace(e, K, e->cw().out_stride));
+    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->cw().src,
                                                    e->err_d);
     heat_solve(e, K, st);
     // u_dev[old][c] = Bh[iperm[old]][c]
-    fcw::launch_permute_rows((int32_t)e->sym.n, k, e->ws.Bh, K, e->iperm_d, u_dev, k, nullptr, st);
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, e->cw().Bh, K, e->iperm_d, u_dev, k, nullptr, st);
     FCW_CUDA(cudaGetLastError());
     return FCW_OK;
 }
@@ -982,11 +1036,11 @@ int fcw_divergence_device(fcw_engine* e, const double* u_dev, int32_t k, double*
     if (k <= 0 || !u_dev || !div_dev) return fail(FCW_E_INVALID, "invalid arguments");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int32_t K = round_k(k);
-    FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
-    FCW_CUDA(cudaMemsetAsync(e->ws.Bh, 0, (size_t)e->sym.n * K * sizeof(double), st));
-    fcw::launch_permute_rows((int32_t)e->sym.n, k, u_dev, k, nullptr, e->ws.Bh, K, e->iperm_d, st);
-    fcw::launch_divergence_fp64(e->fd, e->ws.Bh, e->ws.Bp64, K, st);
-    fcw::launch_permute_rows((int32_t)e->sym.n, k, e->ws.Bp64, K, e->iperm_d, div_dev, k, nullptr, st);
+    FCW_TRY(ensure_workspace(e, K, e->cw().out_stride));
+    FCW_CUDA(cudaMemsetAsync(e->cw().Bh, 0, (size_t)e->sym.n * K * sizeof(double), st));
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, u_dev, k, nullptr, e->cw().Bh, K, e->iperm_d, st);
+    fcw::launch_divergence_fp64(e->fd, e->cw().Bh, e->cw().Bp64, K, st);
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, e->cw().Bp64, K, e->iperm_d, div_dev, k, nullptr, st);
     FCW_CUDA(cudaGetLastError());
     return FCW_OK;
 }
@@ -997,16 +1051,16 @@ int fcw_poisson_solve_device(fcw_engine* e, const double* div_dev, const int32_t
     if (k <= 0 || !div_dev || !sources_dev || !phi_dev) return fail(FCW_E_INVALID, "invalid arguments");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int32_t K = round_k(k);
-    FCW_TRY(ensure_workspace(e, K, e->ws.out_stride));
-    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->ws.src,
+    FCW_TRY(ensure_workspace(e, K, e->cw().out_stride));
+    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->cw().src,
                                                    e->err_d);
-    FCW_CUDA(cudaMemsetAsync(e->ws.Bp64, 0, (size_t)e->sym.n * K * sizeof(double), st));
-    fcw::launch_permute_rows((int32_t)e->sym.n, k, div_dev, k, nullptr, e->ws.Bp64, K, e->iperm_d, st);
-    poisson_solve<double>(e, e->val_p, e->inv_p, e->ws.Bp64, e->ws.Y, K, st);
-    fcw::launch_shift_transpose<double, double>((int32_t)e->sym.n, K, e->ws.Y, e->ws.src, e->ws.dT64, st);
+    FCW_CUDA(cudaMemsetAsync(e->cw().Bp64, 0, (size_t)e->sym.n * K * sizeof(double), st));
+    fcw::launch_permute_rows((int32_t)e->sym.n, k, div_dev, k, nullptr, e->cw().Bp64, K, e->iperm_d, st);
+    poisson_solve<double>(e, e->val_p, e->inv_p, e->cw().Bp64, e->cw().Y, K, st);
+    fcw::launch_shift_transpose<double, double>((int32_t)e->sym.n, K, e->cw().Y, e->cw().src, e->cw().dT64, st);
     // phi_dev[old][c] = dT[c][iperm[old]]: transpose back through the permute kernel, column by column
     for (int32_t c = 0; c < k; ++c)
-        fcw::launch_permute_rows((int32_t)e->sym.n, 1, e->ws.dT64 + (int64_t)c * e->sym.n, 1, e->iperm_d,
+        fcw::launch_permute_rows((int32_t)e->sym.n, 1, e->cw().dT64 + (int64_t)c * e->sym.n, 1, e->iperm_d,
                                  phi_dev + c, k, nullptr, st);
     FCW_CUDA(cudaGetLastError());
     return FCW_OK;
@@ -1024,11 +1078,11 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
     fcw::MetricArgs a;
     FCW_TRY(metric_args(e, targets, nt, nb, eps, K, a));
     a.out = out_dev;
-    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->ws.src,
+    k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->cw().src,
                                                    e->err_d);
-    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)e->sym.n, k, K, d_dev, e->iperm_d, e->ws.Y);
-    fcw::launch_shift_stats<double, double>(a, K, e->ws.Y, e->ws.dT64, st);
-    metrics_block<double>(e, a, e->ws.dT64, st);
+    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)e->sym.n, k, K, d_dev, e->iperm_d, e->cw().Y);
+    fcw::launch_shift_stats<double, double>(a, K, e->cw().Y, e->cw().dT64, st);
+    metrics_block<double>(e, a, e->cw().dT64, st);
     FCW_CUDA(cudaGetLastError());
     return FCW_OK;
 }

@@ -27,7 +27,7 @@ DEFAULT_DIFFUSION_LENGTH_MM = 0.7          # distance_engines.py:12
 MIN_DIFFUSION_LENGTH_MM = 0.5              # distance_engines.py:13
 RECOMMENDED_MIN_DIFFUSION_LENGTH_MM = 0.7  # distance_engines.py:14
 
-ENGINE_DEFAULTS = dict(block_k=1024, leaf_size=64, max_width=64, relax=32, build_mixed=1, device=0, refine_steps=0)
+ENGINE_DEFAULTS = dict(block_k=1024, leaf_size=64, max_width=64, relax=32, build_mixed=1, device=0, pipeline_depth=2)
 
 
 class HeatEngine:
@@ -172,7 +172,7 @@ class B200DistanceEngine(BaseDistanceEngine):
     `allow_eigen_fallback` is accepted and ignored (there is no SuiteSparse
     backend to check). The engine has no intrinsic-Delaunay ("robust")
     operators, so `use_robust=True` raises instead of being silently ignored. Other keys are engine tunables (block_k,
-    leaf_size, max_width, relax, build_mixed, device, refine_steps).
+    leaf_size, max_width, relax, build_mixed, device, pipeline_depth).
 
     The operators are the extrinsic cotan Laplacian L = G^T diag(A) G and the
     barycentric lumped mass (fastcw_lean.py:394-413), so `use_robust` is False.
