@@ -164,6 +164,7 @@ def _config(args, pm):
     return {"workload": f"{args.workload} folded icosphere, {pm.n_vertices} cortical sources, "
                         f"{pm.n_faces} faces, t=(0.7 mm)^2, 12 scales + {N_BETWEEN} samples between",
             "batch_sources_per_step": args.batch, "block_k": args.block_k, "precision": args.precision,
+            "pipeline_depth": args.pipeline_depth,
             "parallelism": f"replicas{args.gpus}", "l2": "inputs larger than L2 (n x K RHS blocks > 126 MB)"}
 
 
@@ -264,7 +265,7 @@ def run_gpu(args):
     _, pm = _mesh(args.workload, args.seed)
     targets = pm.targets(M.RUNNER_SCALES)
     t0 = time.perf_counter()
-    eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k)
+    eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k, pipeline_depth=args.pipeline_depth)
     build_s = time.perf_counter() - t0
     info = eng.info()
 
@@ -460,6 +461,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=4096, help="sources per step")
     ap.add_argument("--block-k", type=int, default=1024)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--pipeline-depth", type=int, default=2, help="blocks in flight on separate streams")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=24, help="sources timed on the CPU oracle (0 = skip)")
     ap.add_argument("--cpu-timeout", type=float, default=600.0)

@@ -6,8 +6,10 @@
 // place. R is never written, because several CTAs of one supernode (its row
 // chunks) each rebuild that supernode's right-hand side. A CTA
 // owns one task of one supernode and a 64-column tile of the right-hand sides;
-// all dense work is 64 x 64 register-tiled products staged in shared memory
-// (256 threads, 4 x 4 outputs per thread).
+// all dense work is register-tiled products staged in shared memory (256
+// threads; a thread owns 4 rows x KT/16 columns). Column tiles are 64 wide in
+// FP64 and 128 wide in FP32; the inverse diagonal block and the panel chunk of
+// a forward task arrive by cp.async while the children's updates are gathered.
 //
 // Forward (leaves -> root), multifrontal: supernode s forms
 //   W   = b_s - sum of the children's update rows that land on s's columns
@@ -34,198 +36,240 @@ namespace fcw {
 namespace {
 
 constexpr int TR = kMaxWidth;   // rows of a tile (= widest supernode)
-constexpr int KT = kRhsTile;    // right-hand sides per CTA
-constexpr int LDS = KT + 1;
-constexpr int LDP = TR + 1;
+constexpr int LDP = TR + 1;     // leading dimension of panel / inverse tiles
 constexpr int RC = 32;          // structure rows per staged chunk in the backward gather
 constexpr int kGatherStage = 1024;  // gather entries staged in shared memory per forward task
 
-template <typename T>
-__device__ __forceinline__ void zero(T (&acc)[4][4]) {
+template <typename T, int NB>
+__device__ __forceinline__ void zero(T (&acc)[4][NB]) {
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = T(0);
+        for (int b = 0; b < NB; ++b) acc[a][b] = T(0);
 }
 
-// acc[a][b] += sum_{j<depth} A[(ty+16a)*lda + j] * Bm[j*ldb + tx+16b]   (A rows, B rows in smem)
-template <typename T>
-__device__ __forceinline__ void mma_rows(T (&acc)[4][4], const T* A, int lda, const T* Bm, int ldb, int depth,
+// acc[a][b] += sum_{j<depth} A[(ty+16a)*lda + j] * Bm[j*ldb + tx+16b]
+template <typename T, int NB>
+__device__ __forceinline__ void mma_rows(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
                                          int ty, int tx) {
     for (int j = 0; j < depth; ++j) {
-        T w[4];
+        T w[NB];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) w[b] = Bm[j * ldb + tx + 16 * b];
+        for (int b = 0; b < NB; ++b) w[b] = Bm[j * ldb + tx + 16 * b];
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const T l = A[(ty + 16 * a) * lda + j];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] += l * w[b];
+            for (int b = 0; b < NB; ++b) acc[a][b] += l * w[b];
         }
     }
 }
 
 // acc[a][b] += sum_{j<depth} A[j*lda + ty+16a] * Bm[j*ldb + tx+16b]   (A transposed)
-template <typename T>
-__device__ __forceinline__ void mma_cols(T (&acc)[4][4], const T* A, int lda, const T* Bm, int ldb, int depth,
+template <typename T, int NB>
+__device__ __forceinline__ void mma_cols(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
                                          int ty, int tx) {
     for (int j = 0; j < depth; ++j) {
-        T w[4], l[4];
+        T w[NB], l[4];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) w[b] = Bm[j * ldb + tx + 16 * b];
+        for (int b = 0; b < NB; ++b) w[b] = Bm[j * ldb + tx + 16 * b];
 #pragma unroll
         for (int a = 0; a < 4; ++a) l[a] = A[j * lda + ty + 16 * a];
 #pragma unroll
         for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] += l[a] * w[b];
+            for (int b = 0; b < NB; ++b) acc[a][b] += l[a] * w[b];
     }
 }
 
-// rows [f0, f0+nf) of supernode s's front (fb = its first front row): out[r][c] =
-// init(r, k) + sign * sum of the children's update rows listed for front row f0+r,
-// for this CTA's 64 columns. Entries are staged in shared memory when they fit;
-// each thread owns one column and every 4th row, so its loads are independent.
-template <typename T, typename Init>
-__device__ __forceinline__ void gather_rows(const SolveArgs<T>& a, int64_t fb, int f0, int nrows, T* out, Init init,
-                                            T sign, int* gsrc, int* gchild, int* grs) {
-    const int tid = threadIdx.x;
-    const int K = a.K, k0 = blockIdx.y * KT;
-    const int eb = a.gm_ptr[fb + f0];
-    const int E = a.gm_ptr[fb + f0 + nrows] - eb;
-    const bool staged = E <= kGatherStage;
-    for (int r = tid; r <= nrows; r += 256) grs[r] = a.gm_ptr[fb + f0 + r] - eb;
-    if (staged)
-        for (int e = tid; e < E; e += 256) {
-            gsrc[e] = a.gm_src[eb + e];
-            gchild[e] = a.gm_child[eb + e];
-        }
-    __syncthreads();
-    const int c = tid & (KT - 1), k = k0 + c;
-    for (int r = tid / KT; r < nrows; r += 256 / KT) {
-        T v = init(r, k);
-        const int e0 = grs[r], e1 = grs[r + 1];
-        for (int e = e0; e < e1; ++e) {
-            const int src = staged ? gsrc[e] : a.gm_src[eb + e];
-            const int ch = staged ? gchild[e] : a.gm_child[eb + e];
-            if (a.reach && !a.reach[ch]) continue;
-            v += sign * a.U[(int64_t)src * K + k];
-        }
-        out[r * LDS + c] = v;
-    }
-    __syncthreads();
+// Asynchronous global -> shared copy of one element (cp.async, L1-allocating).
+template <typename T>
+__device__ __forceinline__ void copy_async(T* smem, const T* gmem) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Gather lists of front rows [f0, f0+nrows) of the supernode whose first front row
+// is fb: each front row lists the children's update rows that land on it. The
+// entries of consecutive rows are contiguous; they are staged in shared memory
+// when they fit (staged = true), otherwise read from global memory.
+struct Gather {
+    int eb;
+    bool staged;
+};
 
 template <typename T>
+__device__ __forceinline__ Gather stage_entries(const SolveArgs<T>& a, int64_t fb, int f0, int nrows, int* gsrc,
+                                                int* gchild, int* grs) {
+    const int tid = threadIdx.x;
+    Gather g;
+    g.eb = a.gm_ptr[fb + f0];
+    const int E = a.gm_ptr[fb + f0 + nrows] - g.eb;
+    g.staged = E <= kGatherStage;
+    for (int r = tid; r <= nrows; r += 256) grs[r] = a.gm_ptr[fb + f0 + r] - g.eb;
+    if (g.staged)
+        for (int e = tid; e < E; e += 256) {
+            gsrc[e] = a.gm_src[g.eb + e];
+            gchild[e] = a.gm_child[g.eb + e];
+        }
+    __syncthreads();
+    return g;
+}
+
+// Sum of the listed children's update rows for front row r (relative), column k.
+template <typename T>
+__device__ __forceinline__ T gathered(const SolveArgs<T>& a, const Gather& g, int r, int k, const int* gsrc,
+                                      const int* gchild, const int* grs) {
+    T v = T(0);
+    for (int e = grs[r]; e < grs[r + 1]; ++e) {
+        const int src = g.staged ? gsrc[e] : a.gm_src[g.eb + e];
+        const int ch = g.staged ? gchild[e] : a.gm_child[g.eb + e];
+        if (a.reach && !a.reach[ch]) continue;
+        v += a.U[(int64_t)src * a.K + k];
+    }
+    return v;
+}
+
+template <typename T, int KTT>
 __global__ void __launch_bounds__(256) k_fwd(SolveArgs<T> a, int32_t t0) {
+    constexpr int NB = KTT / 16, LDW = KTT + 1;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* Ws = reinterpret_cast<T*>(smraw);   // TR x LDS
-    T* Xs = Ws + TR * LDS;                  // TR x LDS
-    T* Ms = Xs + TR * LDS;                  // TR x LDP
+    T* Wt = reinterpret_cast<T*>(smraw);   // TR x LDW: W, then X
+    T* Li = Wt + TR * LDW;                  // TR x LDP: inverse diagonal block
+    T* Pn = Li + TR * LDP;                  // TR x LDP: panel rows of this chunk
     __shared__ int gsrc[kGatherStage], gchild[kGatherStage], grs[TR + 1];
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, chunk = task.y;
     if (a.reach && !a.reach[s]) return;
     const DevPlan& p = a.p;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int ty = tid >> 4, tx = tid & 15;
-    const int K = a.K, k0 = blockIdx.y * KT;
+    const int K = a.K, k0 = blockIdx.y * KTT;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, m = p.sn_m[s], nr = m - ns;
     const int64_t fb = p.sn_rowptr[s];
+    const int q0 = chunk * TR;
+    const int nq = nr > 0 ? min(TR, nr - q0) : 0;
 
-    // W = right-hand side of s's columns minus the children's updates on them.
-    // The gather entries of these rows are contiguous; stage them in shared memory
-    // so every (row, column) accumulation issues independent, coalesced loads.
-    gather_rows<T>(a, fb, 0, ns, Ws, [&](int f, int k) -> T {
-        if (a.delta_src) return (a.delta_src[k] == c0 + f) ? T(1) : T(0);
-        return a.R[(int64_t)(c0 + f) * K + k];
-    }, T(-1), gsrc, gchild, grs);
+    // the inverse block and this chunk's panel rows stream in while the gather runs
     const T* inv = a.inv + p.sn_invptr[s];
     for (int e = tid; e < ns * ns; e += 256) {
         const int i = e / ns, j = e - i * ns;
-        Ms[i * LDP + j] = inv[e];
+        copy_async(&Li[i * LDP + j], inv + e);
     }
-    __syncthreads();
-    T acc[4][4];
+    const T* P = a.val + p.sn_valptr[s] + (int64_t)(ns + q0) * ns;
+    for (int e = tid; e < nq * ns; e += 256) {
+        const int r = e / ns, j = e - r * ns;
+        copy_async(&Pn[r * LDP + j], P + e);
+    }
+
+    // W = right-hand side of s's columns (identity columns are built in place,
+    // stored ones arrive by cp.async with the blocks above), then minus the
+    // children's updates on them
+    if (a.delta_src) {
+        for (int e = tid; e < ns * KTT; e += 256) {
+            const int f = e / KTT, c = e - f * KTT;
+            Wt[f * LDW + c] = (a.delta_src[k0 + c] == c0 + f) ? T(1) : T(0);
+        }
+    } else {
+        for (int e = tid; e < ns * KTT; e += 256) {
+            const int f = e / KTT, c = e - f * KTT;
+            copy_async(&Wt[f * LDW + c], a.R + (int64_t)(c0 + f) * K + k0 + c);
+        }
+    }
+    copy_async_commit();
+    {
+        const Gather g = stage_entries(a, fb, 0, ns, gsrc, gchild, grs);  // ends with a barrier
+        copy_async_wait();
+        __syncthreads();
+        if (grs[ns] > 0) {  // some child update lands on these rows
+            const int c = tid % KTT, k = k0 + c;
+            for (int f = tid / KTT; f < ns; f += 256 / KTT)
+                if (grs[f + 1] > grs[f]) Wt[f * LDW + c] -= gathered(a, g, f, k, gsrc, gchild, grs);
+            __syncthreads();
+        }
+    }
+    // X = inv(L_ss) W, written over W
+    T acc[4][NB];
     zero(acc);
-    mma_rows(acc, Ms, LDP, Ws, LDS, ns, ty, tx);
+    mma_rows(acc, Li, LDP, Wt, LDW, ns, ty, tx);
+    __syncthreads();
 #pragma unroll
     for (int aa = 0; aa < 4; ++aa) {
         const int t = ty + 16 * aa;
         if (t < ns)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) Xs[t * LDS + tx + 16 * b] = acc[aa][b];
+            for (int b = 0; b < NB; ++b) Wt[t * LDW + tx + 16 * b] = acc[aa][b];
     }
     __syncthreads();
-    if (chunk == 0) {
-        for (int t = warp; t < ns; t += 8) {
-            a.B[(int64_t)(c0 + t) * K + k0 + lane] = Xs[t * LDS + lane];
-            a.B[(int64_t)(c0 + t) * K + k0 + lane + 32] = Xs[t * LDS + lane + 32];
+    if (chunk == 0)
+        for (int e = tid; e < ns * KTT; e += 256) {
+            const int t = e / KTT, c = e - t * KTT;
+            a.B[(int64_t)(c0 + t) * K + k0 + c] = Wt[t * LDW + c];
         }
-    }
-    if (nr == 0) return;
-    const int q0 = chunk * TR;
-    const int nq = min(TR, nr - q0);
-    const T* P = a.val + p.sn_valptr[s] + (int64_t)(ns + q0) * ns;
-    for (int e = tid; e < nq * ns; e += 256) {
-        const int r = e / ns, j = e - r * ns;
-        Ms[r * LDP + j] = P[e];
-    }
-    __syncthreads();
+    if (nq <= 0) return;
+    // U_s rows of this chunk = L_rs X + the children's updates landing on them
+    const Gather g = stage_entries(a, fb, ns + q0, nq, gsrc, gchild, grs);
     zero(acc);
-    mma_rows(acc, Ms, LDP, Xs, LDS, ns, ty, tx);
+    mma_rows(acc, Pn, LDP, Wt, LDW, ns, ty, tx);
+    T* Us = a.U + (a.uoff[s] + q0) * (int64_t)K;
 #pragma unroll
     for (int aa = 0; aa < 4; ++aa) {
         const int r = ty + 16 * aa;
         if (r < nq)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) Ws[r * LDS + tx + 16 * b] = acc[aa][b];
-    }
-    __syncthreads();
-    // U_s rows of this chunk = L_rs X_s (in Ws) + the children's updates landing on them
-    gather_rows<T>(a, fb, ns + q0, nq, Ws, [&](int r, int k) -> T { return Ws[r * LDS + (k - k0)]; }, T(1), gsrc,
-                   gchild, grs);
-    T* Us = a.U + (a.uoff[s] + q0) * (int64_t)K;
-    for (int e = tid; e < nq * KT; e += 256) {
-        const int r = e / KT, c = e - r * KT;
-        Us[(int64_t)r * K + k0 + c] = Ws[r * LDS + c];
+            for (int b = 0; b < NB; ++b) {
+                const int k = k0 + tx + 16 * b;
+                Us[(int64_t)r * K + k] = acc[aa][b] + gathered(a, g, r, k, gsrc, gchild, grs);
+            }
     }
 }
 
-template <typename T>
+template <typename T, int KTT>
 __global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
+    constexpr int NB = KTT / 16, LDW = KTT + 1;
+    static_assert(RC * LDP + RC * LDW >= TR * LDP, "the inverse tile aliases the gather staging area");
     extern __shared__ __align__(16) unsigned char smraw[];
     T* Ps = reinterpret_cast<T*>(smraw);   // RC x LDP  panel rows of the chunk
-    T* Xg = Ps + RC * LDP;                  // RC x LDS  gathered solution rows
-    T* Cs = Xg + RC * LDS;                  // TR x LDS
+    T* Xg = Ps + RC * LDP;                  // RC x LDW  gathered solution rows
+    T* Cs = Xg + RC * LDW;                  // TR x LDW
     T* Ms = Ps;                             // TR x LDP  inverse diagonal block, after the gather
     __shared__ int last_arrival;
+    __shared__ int rsh[RC];
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, split = task.y;
     const DevPlan& p = a.p;
     const int tid = threadIdx.x;
     const int ty = tid >> 4, tx = tid & 15;
-    const int K = a.K, k0 = blockIdx.y * KT;
+    const int K = a.K, k0 = blockIdx.y * KTT;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, m = p.sn_m[s], nr = m - ns;
     const int nspl = a.nsplit[s];
     const int q0 = split * kSplitRows, q1 = min(nr, q0 + kSplitRows);
     const T* P = a.val + p.sn_valptr[s];
     const int32_t* rows = p.rows + p.sn_rowptr[s];
 
-    T acc[4][4];
+    T acc[4][NB];
     zero(acc);
     for (int qq = q0; qq < q1; qq += RC) {
         const int nc = min(RC, q1 - qq);
+        if (tid < nc) rsh[tid] = rows[ns + qq + tid];
         for (int e = tid; e < nc * ns; e += 256) {
             const int r = e / ns, j = e - r * ns;
-            Ps[r * LDP + j] = P[(int64_t)(ns + qq + r) * ns + j];
-        }
-        for (int e = tid; e < nc * KT; e += 256) {
-            const int r = e / KT, c = e - r * KT;
-            Xg[r * LDS + c] = a.B[(int64_t)rows[ns + qq + r] * K + k0 + c];
+            copy_async(&Ps[r * LDP + j], P + (int64_t)(ns + qq + r) * ns + j);
         }
         __syncthreads();
-        mma_cols(acc, Ps, LDP, Xg, LDS, nc, ty, tx);
+        for (int e = tid; e < nc * KTT; e += 256) {
+            const int r = e / KTT, c = e - r * KTT;
+            copy_async(&Xg[r * LDW + c], a.B + (int64_t)rsh[r] * K + k0 + c);
+        }
+        copy_async_commit();
+        copy_async_wait();
+        __syncthreads();
+        mma_cols(acc, Ps, LDP, Xg, LDW, nc, ty, tx);
         __syncthreads();
     }
 
@@ -237,7 +281,7 @@ __global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
             const int t = ty + 16 * aa;
             if (t < ns)
 #pragma unroll
-                for (int b = 0; b < 4; ++b)
+                for (int b = 0; b < NB; ++b)
                     part[((int64_t)split * TR + t) * K + k0 + tx + 16 * b] = acc[aa][b];
         }
         __threadfence();
@@ -254,7 +298,7 @@ __global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
             const int t = ty + 16 * aa;
             if (t < ns)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
+                for (int b = 0; b < NB; ++b) {
                     T sum = T(0);
                     for (int sp = 0; sp < nspl; ++sp)
                         sum += __ldcg(&part[((int64_t)sp * TR + t) * K + k0 + tx + 16 * b]);
@@ -268,10 +312,10 @@ __global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
         const int t = ty + 16 * aa;
         if (t < ns)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
+            for (int b = 0; b < NB; ++b) {
                 const int c = tx + 16 * b;
                 const T y = zero_y ? T(0) : a.B[(int64_t)(c0 + t) * K + k0 + c];
-                Cs[t * LDS + c] = y - acc[aa][b];
+                Cs[t * LDW + c] = y - acc[aa][b];
             }
     }
     const T* inv = a.inv + p.sn_invptr[s];
@@ -281,13 +325,13 @@ __global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
     }
     __syncthreads();
     zero(acc);
-    mma_cols(acc, Ms, LDP, Cs, LDS, ns, ty, tx);
+    mma_cols(acc, Ms, LDP, Cs, LDW, ns, ty, tx);
 #pragma unroll
     for (int aa = 0; aa < 4; ++aa) {
         const int t = ty + 16 * aa;
         if (t < ns)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) a.B[(int64_t)(c0 + t) * K + k0 + tx + 16 * b] = acc[aa][b];
+            for (int b = 0; b < NB; ++b) a.B[(int64_t)(c0 + t) * K + k0 + tx + 16 * b] = acc[aa][b];
     }
 }
 
@@ -305,35 +349,50 @@ __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __res
     }
 }
 
+template <typename T, int KTT>
+constexpr size_t fwd_smem() { return (size_t)(TR * (KTT + 1) + 2 * TR * LDP) * sizeof(T); }
+template <typename T, int KTT>
+constexpr size_t bwd_smem() { return (size_t)(RC * LDP + RC * (KTT + 1) + TR * (KTT + 1)) * sizeof(T); }
+
+// Widest column tile each precision uses when K allows it.
 template <typename T>
-constexpr size_t fwd_smem() { return (size_t)(2 * TR * LDS + TR * LDP) * sizeof(T); }
-template <typename T>
-constexpr size_t bwd_smem() { return (size_t)(RC * LDP + RC * LDS + TR * LDS) * sizeof(T); }
-static_assert(RC * LDP + RC * LDS >= TR * LDP, "the inverse tile aliases the gather staging area");
+constexpr int wide_tile() { return sizeof(T) == 4 ? 128 : 64; }
+
+template <typename T, int KTT>
+cudaError_t set_smem() {
+    cudaError_t e = cudaFuncSetAttribute(k_fwd<T, KTT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fwd_smem<T, KTT>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_bwd<T, KTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem<T, KTT>());
+}
 
 }  // namespace
 
 cudaError_t configure_solve_kernels() {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem<double>())))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem<float>())))
-        return e;
-    if ((e = cudaFuncSetAttribute(k_bwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem<double>())))
-        return e;
-    return cudaFuncSetAttribute(k_bwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem<float>());
+    if ((e = set_smem<double, 64>())) return e;
+    if ((e = set_smem<float, 64>())) return e;
+    return set_smem<float, 128>();
 }
 
 template <typename T>
 void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
     if (ntasks <= 0 || a.K <= 0) return;
-    k_fwd<T><<<dim3(ntasks, a.K / KT), 256, fwd_smem<T>(), st>>>(a, t0);
+    constexpr int W = wide_tile<T>();
+    if (W != 64 && a.K % W == 0)
+        k_fwd<T, W><<<dim3(ntasks, a.K / W), 256, fwd_smem<T, W>(), st>>>(a, t0);
+    else
+        k_fwd<T, 64><<<dim3(ntasks, a.K / 64), 256, fwd_smem<T, 64>(), st>>>(a, t0);
 }
 
 template <typename T>
 void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
     if (ntasks <= 0 || a.K <= 0) return;
-    k_bwd<T><<<dim3(ntasks, a.K / KT), 256, bwd_smem<T>(), st>>>(a, t0);
+    constexpr int W = wide_tile<T>();
+    if (W != 64 && a.K % W == 0)
+        k_bwd<T, W><<<dim3(ntasks, a.K / W), 256, bwd_smem<T, W>(), st>>>(a, t0);
+    else
+        k_bwd<T, 64><<<dim3(ntasks, a.K / 64), 256, bwd_smem<T, 64>(), st>>>(a, t0);
 }
 
 void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st) {
