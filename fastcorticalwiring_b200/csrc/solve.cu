@@ -4,27 +4,32 @@
 // contiguous right-hand sides). The forward sweep reads R and writes the
 // forward result into B; the backward sweep turns B into the solution in
 // place. R is never written, because several CTAs of one supernode (its row
-// chunks) each rebuild that supernode's right-hand side. A CTA
-// owns one task of one supernode and a 64-column tile of the right-hand sides;
-// all dense work is register-tiled products staged in shared memory (256
-// threads; a thread owns 4 rows x KT/16 columns). Column tiles are 64 wide in
-// FP64 and 128 wide in FP32; the inverse diagonal block and the panel chunk of
-// a forward task arrive by cp.async while the children's updates are gathered.
+// chunks) each rebuild that supernode's right-hand side.
+//
+// A CTA owns one task of one supernode and one column tile of the right-hand
+// sides (64 columns in FP64, 128 in FP32: a tile row is 512 bytes either way).
+// Every row of a tile is a contiguous 512-byte segment of an n x K array, so
+// all row traffic (right-hand sides, children's update rows, the ancestors'
+// solution rows, results) moves as 16-byte cp.async copies or vector stores,
+// and a CTA issues all the copies of a stage before it waits for any of them.
+// The dense work is register-tiled products staged in shared memory (256
+// threads; a thread owns 4 rows x KT/16 columns in 16-byte groups of
+// adjacent columns, read as vectors).
 //
 // Forward (leaves -> root), multifrontal: supernode s forms
-//   W   = b_s - sum of the children's update rows that land on s's columns
+//   W   = b_s - the children's update rows that land on s's columns
 //   X_s = inv(L_ss) W                                   (written to B)
-//   U_s = (children's update rows that land on s's structure) + L_rs X_s
-// and leaves U_s (nr x K) for its parent. Children are gathered through a
-// per-front-row list in ascending child order, so results are deterministic.
-// A supernode with a long structure is split into 64-row tasks that each
-// recompute X_s (cheap) and write their own rows of U_s.
+//   U_s = L_rs X_s + the children's update rows that land on s's structure
+// and leaves U_s (nr x K) for its parent. Children's rows are listed per front
+// row in ascending child order and added in that order, so results are
+// deterministic. A supernode with a long structure is split into 64-row tasks
+// that each recompute X_s (cheap) and write their own rows of U_s.
 //
 // Backward (root -> leaves): C = y_s - L_rs^T X_r (gather of the structure
-// rows, which belong to ancestors and are final), X_s = inv(L_ss)^T C. Long
-// structures are split over several CTAs (split-K); each writes a partial sum,
-// and the CTA that arrives last (atomic ticket, no waiting) adds the partials in
-// split order and finishes the supernode.
+// rows, which belong to ancestors and are final; two chunks in flight),
+// X_s = inv(L_ss)^T C. Long structures are split over several CTAs (split-K);
+// each writes a partial sum, and the CTA that arrives last (atomic ticket, no
+// waiting) adds the partials in split order and finishes the supernode.
 //
 // Heat right-hand sides are columns of the identity: the forward sweep builds
 // them from the source list, and only supernodes on a source's path to the
@@ -35,10 +40,47 @@ namespace fcw {
 
 namespace {
 
+constexpr int NT = 256;         // threads per CTA
 constexpr int TR = kMaxWidth;   // rows of a tile (= widest supernode)
-constexpr int LDP = TR + 1;     // leading dimension of panel / inverse tiles
-constexpr int RC = 32;          // structure rows per staged chunk in the backward gather
-constexpr int kGatherStage = 1024;  // gather entries staged in shared memory per forward task
+constexpr int LDP = TR + 1;     // leading dimension of the forward inverse / panel tiles
+constexpr int RC = 32;          // structure rows per backward chunk
+
+// Column tile of each precision when K allows it (512-byte rows).
+template <typename T>
+constexpr int wide_tile() { return sizeof(T) == 4 ? 128 : 64; }
+// Children's update rows staged per forward gather chunk (two CTAs per SM).
+template <typename T>
+constexpr int stage_rows() { return sizeof(T) == 4 ? 112 : 88; }
+template <typename T>
+constexpr int vec() { return 16 / (int)sizeof(T); }  // elements per 16-byte vector
+
+// One 16-byte vector (vec<T>() elements) between memory and registers.
+template <typename T>
+__device__ __forceinline__ void ldv(const T* p, T* w) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+    } else {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        w[0] = v.x; w[1] = v.y;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void stv(T* p, const T* w) {
+    if constexpr (sizeof(T) == 4)
+        *reinterpret_cast<float4*>(p) = make_float4(w[0], w[1], w[2], w[3]);
+    else
+        *reinterpret_cast<double2*>(p) = make_double2(w[0], w[1]);
+}
+
+// Column of a thread's b-th accumulator: 16-byte groups of adjacent columns,
+// 16 groups apart, so a half-warp reads 256 contiguous bytes per vector load.
+template <typename T>
+__device__ __forceinline__ int col_of(int tx, int b) {
+    constexpr int G = vec<T>();
+    return G * tx + (b % G) + 16 * G * (b / G);
+}
 
 template <typename T, int NB>
 __device__ __forceinline__ void zero(T (&acc)[4][NB]) {
@@ -48,41 +90,85 @@ __device__ __forceinline__ void zero(T (&acc)[4][NB]) {
         for (int b = 0; b < NB; ++b) acc[a][b] = T(0);
 }
 
-// acc[a][b] += sum_{j<depth} A[(ty+16a)*lda + j] * Bm[j*ldb + tx+16b]
-template <typename T, int NB>
-__device__ __forceinline__ void mma_rows(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
-                                         int ty, int tx) {
+// acc[a][b] += sum_{j<depth} A[(ty+16a)*lda + j] * Bm[j*ldb + col_of(tx,b)], a < NA
+template <typename T, int NB, int NA>
+__device__ __forceinline__ void mma_rows_n(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
+                                           int ty, int tx) {
+    constexpr int G = vec<T>();
+    const T* ap = A + ty * lda;
+    const T* bp = Bm + G * tx;
     for (int j = 0; j < depth; ++j) {
         T w[NB];
 #pragma unroll
-        for (int b = 0; b < NB; ++b) w[b] = Bm[j * ldb + tx + 16 * b];
+        for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            const T l = A[(ty + 16 * a) * lda + j];
+        for (int a = 0; a < NA; ++a) {
+            const T l = ap[16 * a * lda + j];
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc[a][b] += l * w[b];
         }
     }
 }
 
-// acc[a][b] += sum_{j<depth} A[j*lda + ty+16a] * Bm[j*ldb + tx+16b]   (A transposed)
-template <typename T, int NB>
-__device__ __forceinline__ void mma_cols(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
-                                         int ty, int tx) {
+// acc[a][b] += sum_{j<depth} A[j*lda + ty+16a] * Bm[j*ldb + col_of(tx,b)], a < NA   (A transposed)
+template <typename T, int NB, int NA>
+__device__ __forceinline__ void mma_cols_n(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
+                                           int ty, int tx) {
+    constexpr int G = vec<T>();
+    const T* bp = Bm + G * tx;
     for (int j = 0; j < depth; ++j) {
-        T w[NB], l[4];
+        T w[NB], l[NA];
 #pragma unroll
-        for (int b = 0; b < NB; ++b) w[b] = Bm[j * ldb + tx + 16 * b];
+        for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
 #pragma unroll
-        for (int a = 0; a < 4; ++a) l[a] = A[j * lda + ty + 16 * a];
+        for (int a = 0; a < NA; ++a) l[a] = A[j * lda + ty + 16 * a];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc[a][b] += l[a] * w[b];
     }
 }
 
-// Asynchronous global -> shared copy of one element (cp.async, L1-allocating).
+// Only the 16-row blocks that hold one of the first `nrows` rows are computed.
+template <typename T, int NB>
+__device__ __forceinline__ void mma_rows(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
+                                         int nrows, int ty, int tx) {
+    switch ((nrows + 15) >> 4) {
+        case 0: break;
+        case 1: mma_rows_n<T, NB, 1>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+        case 2: mma_rows_n<T, NB, 2>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+        case 3: mma_rows_n<T, NB, 3>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+        default: mma_rows_n<T, NB, 4>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+    }
+}
+
+template <typename T, int NB>
+__device__ __forceinline__ void mma_cols(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
+                                         int nrows, int ty, int tx) {
+    switch ((nrows + 15) >> 4) {
+        case 0: break;
+        case 1: mma_cols_n<T, NB, 1>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+        case 2: mma_cols_n<T, NB, 2>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+        case 3: mma_cols_n<T, NB, 3>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+        default: mma_cols_n<T, NB, 4>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
+    }
+}
+
+// Rows ty+16a < nrows of acc into the row-major tile D (leading dimension ld).
+template <typename T, int NB>
+__device__ __forceinline__ void store_rows(T* D, int64_t ld, const T (&acc)[4][NB], int nrows, int ty, int tx) {
+    constexpr int G = vec<T>();
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int t = ty + 16 * a;
+        if (t < nrows)
+#pragma unroll
+            for (int h = 0; h < NB / G; ++h) stv(D + t * ld + G * tx + 16 * G * h, &acc[a][G * h]);
+    }
+}
+
+// Asynchronous global -> shared copies (cp.async): single elements through L1,
+// 16-byte vectors around it.
 template <typename T>
 __device__ __forceinline__ void copy_async(T* smem, const T* gmem) {
     const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
@@ -91,199 +177,231 @@ __device__ __forceinline__ void copy_async(T* smem, const T* gmem) {
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void copy16_async(void* smem, const void* gmem) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void copy_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// Gather lists of front rows [f0, f0+nrows) of the supernode whose first front row
-// is fb: each front row lists the children's update rows that land on it. The
-// entries of consecutive rows are contiguous; they are staged in shared memory
-// when they fit (staged = true), otherwise read from global memory.
-struct Gather {
-    int eb;
-    bool staged;
+// Rows [0, nrows) of a KT-wide shared tile to an n x K array (g = first row, first column).
+template <typename T, int KT>
+__device__ __forceinline__ void tile_rows_to_global(T* g, int64_t K, const T* D, int nrows) {
+    constexpr int VPR = KT / vec<T>();
+    for (int i = threadIdx.x; i < nrows * VPR; i += NT) {
+        const int r = i / VPR, v = i - r * VPR;
+        *reinterpret_cast<uint4*>(g + r * K + v * vec<T>()) =
+            *reinterpret_cast<const uint4*>(D + r * KT + v * vec<T>());
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Children's update rows of front rows [f0, f0+nrows): entries [eb, eb+E) of the
+// gather lists; grs[r] .. grs[r+1] (relative to eb) are those of row r.
+// ---------------------------------------------------------------------------
+struct GatherRange {
+    int eb, E;
 };
 
 template <typename T>
-__device__ __forceinline__ Gather stage_entries(const SolveArgs<T>& a, int64_t fb, int f0, int nrows, int* gsrc,
-                                                int* gchild, int* grs) {
-    const int tid = threadIdx.x;
-    Gather g;
+__device__ __forceinline__ GatherRange gather_open(const SolveArgs<T>& a, int64_t fb, int f0, int nrows, int* grs) {
+    GatherRange g;
     g.eb = a.gm_ptr[fb + f0];
-    const int E = a.gm_ptr[fb + f0 + nrows] - g.eb;
-    g.staged = E <= kGatherStage;
-    for (int r = tid; r <= nrows; r += 256) grs[r] = a.gm_ptr[fb + f0 + r] - g.eb;
-    if (g.staged)
-        for (int e = tid; e < E; e += 256) {
-            gsrc[e] = a.gm_src[g.eb + e];
-            gchild[e] = a.gm_child[g.eb + e];
-        }
-    __syncthreads();
+    g.E = a.gm_ptr[fb + f0 + nrows] - g.eb;
+    for (int r = threadIdx.x; r <= nrows; r += NT) grs[r] = a.gm_ptr[fb + f0 + r] - g.eb;
     return g;
 }
 
-// Sum of the listed children's update rows for front row r (relative), column k.
-template <typename T>
-__device__ __forceinline__ T gathered(const SolveArgs<T>& a, const Gather& g, int r, int k, const int* gsrc,
-                                      const int* gchild, const int* grs) {
-    T v = T(0);
-    for (int e = grs[r]; e < grs[r + 1]; ++e) {
-        const int src = g.staged ? gsrc[e] : a.gm_src[g.eb + e];
-        const int ch = g.staged ? gchild[e] : a.gm_child[g.eb + e];
-        if (a.reach && !a.reach[ch]) continue;
-        v += a.U[(int64_t)src * a.K + k];
+// Async copies of the staged chunk that starts at entry e0; live[e] = 0 for rows
+// of children off the sources' paths (their update rows were never written).
+template <typename T, int KT>
+__device__ __forceinline__ void gather_issue(const SolveArgs<T>& a, const GatherRange& g, int e0, int k0, T* St,
+                                             unsigned char* live) {
+    constexpr int VPR = KT / vec<T>(), SG = stage_rows<T>();
+    const int ne = min(g.E - e0, SG);
+    for (int i = threadIdx.x; i < ne * VPR; i += NT) {
+        const int e = i / VPR, v = i - e * VPR;
+        const int ge = g.eb + e0 + e;
+        const bool on = !a.reach || a.reach[a.gm_child[ge]];
+        if (v == 0) live[e] = on;
+        if (on) copy16_async(St + e * KT + v * vec<T>(), a.U + (int64_t)a.gm_src[ge] * a.K + k0 + v * vec<T>());
     }
-    return v;
 }
 
-template <typename T, int KTT>
-__global__ void __launch_bounds__(256) k_fwd(SolveArgs<T> a, int32_t t0) {
-    constexpr int NB = KTT / 16, LDW = KTT + 1;
+// D rows (+ or -)= the staged entries [e0, e1) that belong to them, in entry order.
+template <typename T, int KT, bool SUB>
+__device__ __forceinline__ void gather_accumulate(T* D, const T* St, const unsigned char* live, const int* grs,
+                                                  int nrows, int e0, int e1) {
+    constexpr int G = vec<T>(), TPR = KT / G, RG = NT / TPR;  // threads per row (one vector each), rows in parallel
+    const int c = G * (threadIdx.x % TPR);
+    for (int r = threadIdx.x / TPR; r < nrows; r += RG) {
+        const int lo = max(grs[r], e0), hi = min(grs[r + 1], e1);
+        if (lo >= hi) continue;
+        T v[G], u[G];
+        ldv(D + r * KT + c, v);
+        for (int e = lo; e < hi; ++e) {
+            if (!live[e - e0]) continue;
+            ldv(St + (e - e0) * KT + c, u);
+#pragma unroll
+            for (int q = 0; q < G; ++q) v[q] = SUB ? v[q] - u[q] : v[q] + u[q];
+        }
+        stv(D + r * KT + c, v);
+    }
+}
+
+// Waits for every copy this CTA has in flight (the caller has issued the
+// range's first chunk), then adds the range chunk by chunk.
+template <typename T, int KT, bool SUB>
+__device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const GatherRange& g, int k0, T* D, int nrows,
+                                              T* St, unsigned char* live, const int* grs) {
+    constexpr int SG = stage_rows<T>();
+    int e0 = 0;
+    do {
+        if (e0 > 0) {
+            gather_issue<T, KT>(a, g, e0, k0, St, live);
+            copy_async_commit();
+        }
+        copy_async_wait();
+        __syncthreads();
+        if (g.E > 0) gather_accumulate<T, KT, SUB>(D, St, live, grs, nrows, e0, min(g.E, e0 + SG));
+        __syncthreads();
+        e0 += SG;
+    } while (e0 < g.E);
+}
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
+    constexpr int NB = KT / 16, VPR = KT / vec<T>();
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* Wt = reinterpret_cast<T*>(smraw);   // TR x LDW: W, then X
-    T* Li = Wt + TR * LDW;                  // TR x LDP: inverse diagonal block
-    T* Pn = Li + TR * LDP;                  // TR x LDP: panel rows of this chunk
-    __shared__ int gsrc[kGatherStage], gchild[kGatherStage], grs[TR + 1];
+    T* Wt = reinterpret_cast<T*>(smraw);   // TR x KT: W, then X, then this chunk's update rows
+    T* Lp = Wt + TR * KT;                   // TR x LDP: inverse diagonal block, then the panel chunk
+    T* St = Lp + TR * LDP;                  // stage_rows x KT: children's update rows
+    __shared__ int grs[TR + 1];
+    __shared__ unsigned char live[stage_rows<T>()];
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, chunk = task.y;
     if (a.reach && !a.reach[s]) return;
     const DevPlan& p = a.p;
     const int tid = threadIdx.x;
     const int ty = tid >> 4, tx = tid & 15;
-    const int K = a.K, k0 = blockIdx.y * KTT;
+    const int K = a.K, k0 = blockIdx.y * KT;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, m = p.sn_m[s], nr = m - ns;
     const int64_t fb = p.sn_rowptr[s];
     const int q0 = chunk * TR;
     const int nq = nr > 0 ? min(TR, nr - q0) : 0;
 
-    // the inverse block and this chunk's panel rows stream in while the gather runs
+    // the inverse block, the right-hand side rows and the first children's rows
+    // are in flight together (identity right-hand sides are built in place)
     const T* inv = a.inv + p.sn_invptr[s];
-    for (int e = tid; e < ns * ns; e += 256) {
+    for (int e = tid; e < ns * ns; e += NT) {
         const int i = e / ns, j = e - i * ns;
-        copy_async(&Li[i * LDP + j], inv + e);
+        copy_async(&Lp[i * LDP + j], inv + e);
     }
-    const T* P = a.val + p.sn_valptr[s] + (int64_t)(ns + q0) * ns;
-    for (int e = tid; e < nq * ns; e += 256) {
-        const int r = e / ns, j = e - r * ns;
-        copy_async(&Pn[r * LDP + j], P + e);
-    }
-
-    // W = right-hand side of s's columns (identity columns are built in place,
-    // stored ones arrive by cp.async with the blocks above), then minus the
-    // children's updates on them
     if (a.delta_src) {
-        for (int e = tid; e < ns * KTT; e += 256) {
-            const int f = e / KTT, c = e - f * KTT;
-            Wt[f * LDW + c] = (a.delta_src[k0 + c] == c0 + f) ? T(1) : T(0);
+        for (int e = tid; e < ns * KT; e += NT) {
+            const int f = e / KT, c = e - f * KT;
+            Wt[f * KT + c] = (a.delta_src[k0 + c] == c0 + f) ? T(1) : T(0);
         }
     } else {
-        for (int e = tid; e < ns * KTT; e += 256) {
-            const int f = e / KTT, c = e - f * KTT;
-            copy_async(&Wt[f * LDW + c], a.R + (int64_t)(c0 + f) * K + k0 + c);
+        for (int i = tid; i < ns * VPR; i += NT) {
+            const int f = i / VPR, v = i - f * VPR;
+            copy16_async(Wt + f * KT + v * vec<T>(), a.R + (int64_t)(c0 + f) * K + k0 + v * vec<T>());
         }
     }
+    const GatherRange g1 = gather_open(a, fb, 0, ns, grs);
+    if (g1.E > 0) gather_issue<T, KT>(a, g1, 0, k0, St, live);
     copy_async_commit();
-    {
-        const Gather g = stage_entries(a, fb, 0, ns, gsrc, gchild, grs);  // ends with a barrier
-        copy_async_wait();
-        __syncthreads();
-        if (grs[ns] > 0) {  // some child update lands on these rows
-            const int c = tid % KTT, k = k0 + c;
-            for (int f = tid / KTT; f < ns; f += 256 / KTT)
-                if (grs[f + 1] > grs[f]) Wt[f * LDW + c] -= gathered(a, g, f, k, gsrc, gchild, grs);
-            __syncthreads();
-        }
-    }
+    gather_finish<T, KT, true>(a, g1, k0, Wt, ns, St, live, grs);
+
     // X = inv(L_ss) W, written over W
     T acc[4][NB];
     zero(acc);
-    mma_rows(acc, Li, LDP, Wt, LDW, ns, ty, tx);
+    mma_rows(acc, Lp, LDP, Wt, KT, ns, ns, ty, tx);
     __syncthreads();
-#pragma unroll
-    for (int aa = 0; aa < 4; ++aa) {
-        const int t = ty + 16 * aa;
-        if (t < ns)
-#pragma unroll
-            for (int b = 0; b < NB; ++b) Wt[t * LDW + tx + 16 * b] = acc[aa][b];
-    }
+    store_rows(Wt, KT, acc, ns, ty, tx);
     __syncthreads();
-    if (chunk == 0)
-        for (int e = tid; e < ns * KTT; e += 256) {
-            const int t = e / KTT, c = e - t * KTT;
-            a.B[(int64_t)(c0 + t) * K + k0 + c] = Wt[t * LDW + c];
-        }
+    if (chunk == 0) tile_rows_to_global<T, KT>(a.B + (int64_t)c0 * K + k0, K, Wt, ns);
     if (nq <= 0) return;
-    // U_s rows of this chunk = L_rs X + the children's updates landing on them
-    const Gather g = stage_entries(a, fb, ns + q0, nq, gsrc, gchild, grs);
-    zero(acc);
-    mma_rows(acc, Pn, LDP, Wt, LDW, ns, ty, tx);
-    T* Us = a.U + (a.uoff[s] + q0) * (int64_t)K;
-#pragma unroll
-    for (int aa = 0; aa < 4; ++aa) {
-        const int r = ty + 16 * aa;
-        if (r < nq)
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const int k = k0 + tx + 16 * b;
-                Us[(int64_t)r * K + k] = acc[aa][b] + gathered(a, g, r, k, gsrc, gchild, grs);
-            }
+
+    // U_s rows of this chunk = L_rs X + the children's rows landing on them; the
+    // panel rows take the inverse's place
+    const T* P = a.val + p.sn_valptr[s] + (int64_t)(ns + q0) * ns;
+    for (int e = tid; e < nq * ns; e += NT) {
+        const int r = e / ns, j = e - r * ns;
+        copy_async(&Lp[r * LDP + j], P + e);
     }
+    const GatherRange g2 = gather_open(a, fb, ns + q0, nq, grs);
+    if (g2.E > 0) gather_issue<T, KT>(a, g2, 0, k0, St, live);
+    copy_async_commit();
+    copy_async_wait();
+    __syncthreads();
+    zero(acc);
+    mma_rows(acc, Lp, LDP, Wt, KT, ns, nq, ty, tx);
+    __syncthreads();
+    store_rows(Wt, KT, acc, nq, ty, tx);
+    gather_finish<T, KT, false>(a, g2, k0, Wt, nq, St, live, grs);
+    tile_rows_to_global<T, KT>(a.U + (a.uoff[s] + q0) * (int64_t)K + k0, K, Wt, nq);
 }
 
-template <typename T, int KTT>
-__global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
-    constexpr int NB = KTT / 16, LDW = KTT + 1;
-    static_assert(RC * LDP + RC * LDW >= TR * LDP, "the inverse tile aliases the gather staging area");
+template <typename T, int KT>
+__global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
+    constexpr int NB = KT / 16, VPR = KT / vec<T>(), G = vec<T>();
+    constexpr int PS = RC * TR, XS = RC * KT;  // one chunk buffer: panel rows, gathered solution rows
+    static_assert(2 * (PS + XS) >= TR * KT + TR * TR, "the finishing tiles alias the chunk buffers");
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* Ps = reinterpret_cast<T*>(smraw);   // RC x LDP  panel rows of the chunk
-    T* Xg = Ps + RC * LDP;                  // RC x LDW  gathered solution rows
-    T* Cs = Xg + RC * LDW;                  // TR x LDW
-    T* Ms = Ps;                             // TR x LDP  inverse diagonal block, after the gather
+    T* buf = reinterpret_cast<T*>(smraw);
+    T* Cs = buf;             // TR x KT, after the gather
+    T* Ms = buf + TR * KT;   // TR x TR inverse diagonal block, after the gather
     __shared__ int last_arrival;
-    __shared__ int rsh[RC];
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, split = task.y;
     const DevPlan& p = a.p;
     const int tid = threadIdx.x;
     const int ty = tid >> 4, tx = tid & 15;
-    const int K = a.K, k0 = blockIdx.y * KTT;
+    const int K = a.K, k0 = blockIdx.y * KT;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, m = p.sn_m[s], nr = m - ns;
     const int nspl = a.nsplit[s];
     const int q0 = split * kSplitRows, q1 = min(nr, q0 + kSplitRows);
     const T* P = a.val + p.sn_valptr[s];
     const int32_t* rows = p.rows + p.sn_rowptr[s];
 
-    T acc[4][NB];
-    zero(acc);
-    for (int qq = q0; qq < q1; qq += RC) {
-        const int nc = min(RC, q1 - qq);
-        if (tid < nc) rsh[tid] = rows[ns + qq + tid];
-        for (int e = tid; e < nc * ns; e += 256) {
+    // chunk ci of the split's structure rows into buffer ci & 1
+    auto issue = [&](int ci) {
+        const int qq = q0 + ci * RC, nc = min(RC, q1 - qq);
+        T* Ps = buf + (ci & 1) * (PS + XS);
+        T* Xg = Ps + PS;
+        for (int e = tid; e < nc * ns; e += NT) {
             const int r = e / ns, j = e - r * ns;
-            copy_async(&Ps[r * LDP + j], P + (int64_t)(ns + qq + r) * ns + j);
+            copy_async(&Ps[r * TR + j], P + (int64_t)(ns + qq + r) * ns + j);
         }
-        __syncthreads();
-        for (int e = tid; e < nc * KTT; e += 256) {
-            const int r = e / KTT, c = e - r * KTT;
-            copy_async(&Xg[r * LDW + c], a.B + (int64_t)rsh[r] * K + k0 + c);
+        for (int i = tid; i < nc * VPR; i += NT) {
+            const int r = i / VPR, v = i - r * VPR;
+            copy16_async(Xg + r * KT + v * vec<T>(), a.B + (int64_t)rows[ns + qq + r] * K + k0 + v * vec<T>());
         }
         copy_async_commit();
-        copy_async_wait();
+    };
+    T acc[4][NB];
+    zero(acc);
+    const int nchunks = q1 > q0 ? (q1 - q0 + RC - 1) / RC : 0;
+    if (nchunks > 0) issue(0);
+    for (int ci = 0; ci < nchunks; ++ci) {
+        if (ci + 1 < nchunks) {
+            issue(ci + 1);
+            copy_async_wait_prev();
+        } else {
+            copy_async_wait();
+        }
         __syncthreads();
-        mma_cols(acc, Ps, LDP, Xg, LDW, nc, ty, tx);
+        const T* Ps = buf + (ci & 1) * (PS + XS);
+        mma_cols(acc, Ps, TR, Ps + PS, KT, min(RC, q1 - q0 - ci * RC), ns, ty, tx);
         __syncthreads();
     }
 
     const bool zero_y = a.reach && !a.reach[s];
     if (nspl > 1) {
-        T* part = a.part + a.poff[s] * (int64_t)TR * K;
-#pragma unroll
-        for (int aa = 0; aa < 4; ++aa) {
-            const int t = ty + 16 * aa;
-            if (t < ns)
-#pragma unroll
-                for (int b = 0; b < NB; ++b)
-                    part[((int64_t)split * TR + t) * K + k0 + tx + 16 * b] = acc[aa][b];
-        }
+        T* part = a.part + a.poff[s] * (int64_t)TR * K + k0;
+        store_rows(part + (int64_t)split * TR * K, (int64_t)K, acc, ns, ty, tx);
         __threadfence();
         __syncthreads();
         if (tid == 0) {
@@ -301,38 +419,39 @@ __global__ void __launch_bounds__(256) k_bwd(SolveArgs<T> a, int32_t t0) {
                 for (int b = 0; b < NB; ++b) {
                     T sum = T(0);
                     for (int sp = 0; sp < nspl; ++sp)
-                        sum += __ldcg(&part[((int64_t)sp * TR + t) * K + k0 + tx + 16 * b]);
+                        sum += __ldcg(&part[((int64_t)sp * TR + t) * K + col_of<T>(tx, b)]);
                     acc[aa][b] = sum;
                 }
         }
         if (tid == 0) a.counters[(int64_t)s * a.ktiles + blockIdx.y] = 0;
     }
+    // C = y - acc; X_s = inv(L_ss)^T C
+    const T* inv = a.inv + p.sn_invptr[s];
+    for (int e = tid; e < ns * ns; e += NT) {
+        const int i = e / ns, j = e - i * ns;
+        copy_async(&Ms[i * TR + j], inv + e);
+    }
+    copy_async_commit();
 #pragma unroll
     for (int aa = 0; aa < 4; ++aa) {
         const int t = ty + 16 * aa;
         if (t < ns)
 #pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const int c = tx + 16 * b;
-                const T y = zero_y ? T(0) : a.B[(int64_t)(c0 + t) * K + k0 + c];
-                Cs[t * LDW + c] = y - acc[aa][b];
+            for (int h = 0; h < NB / G; ++h) {
+                T y[G];
+#pragma unroll
+                for (int q = 0; q < G; ++q) y[q] = T(0);
+                if (!zero_y) ldv(a.B + (int64_t)(c0 + t) * K + k0 + G * tx + 16 * G * h, y);
+#pragma unroll
+                for (int q = 0; q < G; ++q) y[q] -= acc[aa][G * h + q];
+                stv(Cs + t * KT + G * tx + 16 * G * h, y);
             }
     }
-    const T* inv = a.inv + p.sn_invptr[s];
-    for (int e = tid; e < ns * ns; e += 256) {
-        const int i = e / ns, j = e - i * ns;
-        Ms[i * LDP + j] = inv[e];
-    }
+    copy_async_wait();
     __syncthreads();
     zero(acc);
-    mma_cols(acc, Ms, LDP, Cs, LDW, ns, ty, tx);
-#pragma unroll
-    for (int aa = 0; aa < 4; ++aa) {
-        const int t = ty + 16 * aa;
-        if (t < ns)
-#pragma unroll
-            for (int b = 0; b < NB; ++b) a.B[(int64_t)(c0 + t) * K + k0 + tx + 16 * b] = acc[aa][b];
-    }
+    mma_cols(acc, Ms, TR, Cs, KT, ns, ns, ty, tx);
+    store_rows(a.B + (int64_t)c0 * K + k0, (int64_t)K, acc, ns, ty, tx);
 }
 
 __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __restrict__ parent,
@@ -349,21 +468,17 @@ __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __res
     }
 }
 
-template <typename T, int KTT>
-constexpr size_t fwd_smem() { return (size_t)(TR * (KTT + 1) + 2 * TR * LDP) * sizeof(T); }
-template <typename T, int KTT>
-constexpr size_t bwd_smem() { return (size_t)(RC * LDP + RC * (KTT + 1) + TR * (KTT + 1)) * sizeof(T); }
+template <typename T, int KT>
+constexpr size_t fwd_smem() { return (size_t)(TR * KT + TR * LDP + stage_rows<T>() * KT) * sizeof(T); }
+template <typename T, int KT>
+constexpr size_t bwd_smem() { return (size_t)2 * (RC * TR + RC * KT) * sizeof(T); }
 
-// Widest column tile each precision uses when K allows it.
-template <typename T>
-constexpr int wide_tile() { return sizeof(T) == 4 ? 128 : 64; }
-
-template <typename T, int KTT>
+template <typename T, int KT>
 cudaError_t set_smem() {
-    cudaError_t e = cudaFuncSetAttribute(k_fwd<T, KTT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)fwd_smem<T, KTT>());
+    cudaError_t e = cudaFuncSetAttribute(k_fwd<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fwd_smem<T, KT>());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_bwd<T, KTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem<T, KTT>());
+    return cudaFuncSetAttribute(k_bwd<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem<T, KT>());
 }
 
 }  // namespace
@@ -380,9 +495,9 @@ void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStr
     if (ntasks <= 0 || a.K <= 0) return;
     constexpr int W = wide_tile<T>();
     if (W != 64 && a.K % W == 0)
-        k_fwd<T, W><<<dim3(ntasks, a.K / W), 256, fwd_smem<T, W>(), st>>>(a, t0);
+        k_fwd<T, W><<<dim3(ntasks, a.K / W), NT, fwd_smem<T, W>(), st>>>(a, t0);
     else
-        k_fwd<T, 64><<<dim3(ntasks, a.K / 64), 256, fwd_smem<T, 64>(), st>>>(a, t0);
+        k_fwd<T, 64><<<dim3(ntasks, a.K / 64), NT, fwd_smem<T, 64>(), st>>>(a, t0);
 }
 
 template <typename T>
@@ -390,9 +505,9 @@ void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStr
     if (ntasks <= 0 || a.K <= 0) return;
     constexpr int W = wide_tile<T>();
     if (W != 64 && a.K % W == 0)
-        k_bwd<T, W><<<dim3(ntasks, a.K / W), 256, bwd_smem<T, W>(), st>>>(a, t0);
+        k_bwd<T, W><<<dim3(ntasks, a.K / W), NT, bwd_smem<T, W>(), st>>>(a, t0);
     else
-        k_bwd<T, 64><<<dim3(ntasks, a.K / 64), 256, bwd_smem<T, 64>(), st>>>(a, t0);
+        k_bwd<T, 64><<<dim3(ntasks, a.K / 64), NT, bwd_smem<T, 64>(), st>>>(a, t0);
 }
 
 void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st) {
