@@ -42,6 +42,17 @@ METRIC = "sources/s @164k verts"
 N_BETWEEN = 3
 L2_BYTES = 126 * 1024 * 1024
 
+# DRAM bytes (read + write) per 1024-source block of each stage on the L7 mixed
+# workload, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum
+# summed over the stage's launches); profiles/dram_L7_block1024_mixed.md has the
+# command and the per-kernel table. Other configurations report null.
+NCU_TRAFFIC = {
+    ("L7", 1024, "mixed"): {
+        "heat_fwd": 0.170e9, "heat_bwd": 3.858e9, "divergence": 1.904e9, "poisson_fwd": 4.109e9,
+        "poisson_bwd": 2.234e9, "shift": 1.286e9, "metrics": 0.342e9,
+    },
+}
+
 
 def _peaks():
     try:
@@ -357,7 +368,9 @@ def run_gpu(args):
             byts = _stage_bytes(dom, pm.n_vertices, pm.n_faces, args.block_k, info["nnz_factor"], args.precision)
             ach = byts / per_block_s / 1e9
             roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
-                    "frac": ach / hbm, "traffic": None, "peak_kind": peak_kind,
+                    "frac": ach / hbm,
+                    "traffic": NCU_TRAFFIC.get((args.workload, args.block_k, args.precision), {}).get(dom),
+                    "peak_kind": peak_kind,
                     "bytes_per_launch": byts, "launch": f"one {dom} stage on a {args.block_k}-source block"}
         line = {
             "metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
