@@ -12,9 +12,12 @@
 // all row traffic (right-hand sides, children's update rows, the ancestors'
 // solution rows, results) moves as 16-byte cp.async copies or vector stores,
 // and a CTA issues all the copies of a stage before it waits for any of them.
-// The dense work is register-tiled products staged in shared memory (256
-// threads; a thread owns 4 rows x KT/16 columns in 16-byte groups of
-// adjacent columns, read as vectors).
+//
+// Dense products run on shared-memory tiles. FP64 uses the FP64 tensor path
+// (mma.sync m8n8k4: one instruction per 256 multiply-adds; each of the 8 warps
+// owns 8 columns and walks the 8-row tiles the supernode needs). FP32 uses
+// register tiles on the FMA pipes (a thread owns 4 rows x KT/16 columns in
+// 16-byte column groups).
 //
 // Forward (leaves -> root), multifrontal: supernode s forms
 //   W   = b_s - the children's update rows that land on s's columns
@@ -42,7 +45,6 @@ namespace {
 
 constexpr int NT = 256;         // threads per CTA
 constexpr int TR = kMaxWidth;   // rows of a tile (= widest supernode)
-constexpr int LDP = TR + 1;     // leading dimension of the forward inverse / panel tiles
 constexpr int RC = 32;          // structure rows per backward chunk
 
 // Column tile of each precision when K allows it (512-byte rows).
@@ -50,9 +52,22 @@ template <typename T>
 constexpr int wide_tile() { return sizeof(T) == 4 ? 128 : 64; }
 // Children's update rows staged per forward gather chunk (two CTAs per SM).
 template <typename T>
-constexpr int stage_rows() { return sizeof(T) == 4 ? 112 : 88; }
+constexpr int stage_rows() { return sizeof(T) == 4 ? 112 : 80; }
 template <typename T>
 constexpr int vec() { return 16 / (int)sizeof(T); }  // elements per 16-byte vector
+
+// Shared-tile leading dimensions, chosen so that the product's operand reads
+// are free of bank conflicts: FP64 tensor fragments read 8 rows x 4 depths
+// (row stride 68 doubles = 8 banks apart), FP32 register tiles read rows ty and
+// ty+1 of a row-major A (odd stride) or adjacent columns of a transposed one.
+template <typename T>
+constexpr int ld_fwd_a() { return sizeof(T) == 8 ? 68 : TR + 1; }  // forward inverse / panel, row-major
+template <typename T>
+constexpr int ld_bwd_a() { return sizeof(T) == 8 ? 68 : TR; }      // backward panel / inverse, transposed
+template <typename T, int KT>
+constexpr int ld_rows() { return sizeof(T) == 8 ? KT + 4 : KT; }    // right-hand-side rows (W, X, C, gathers)
+template <typename T>
+constexpr int depth_pad() { return sizeof(T) == 8 ? 4 : 1; }        // product depth granularity
 
 // One 16-byte vector (vec<T>() elements) between memory and registers.
 template <typename T>
@@ -74,96 +89,208 @@ __device__ __forceinline__ void stv(T* p, const T* w) {
         *reinterpret_cast<double2*>(p) = make_double2(w[0], w[1]);
 }
 
-// Column of a thread's b-th accumulator: 16-byte groups of adjacent columns,
-// 16 groups apart, so a half-warp reads 256 contiguous bytes per vector load.
-template <typename T>
-__device__ __forceinline__ int col_of(int tx, int b) {
-    constexpr int G = vec<T>();
-    return G * tx + (b % G) + 16 * G * (b / G);
+// V adjacent elements (V * sizeof(T) is 8 or 16 bytes, aligned).
+template <typename T, int V>
+__device__ __forceinline__ void ld_n(const T* p, T* w) {
+    if constexpr (V * sizeof(T) == 16) {
+        ldv(p, w);
+    } else {
+        static_assert(V == 2 && sizeof(T) == 4, "8-byte groups are float pairs");
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        w[0] = v.x; w[1] = v.y;
+    }
+}
+template <typename T, int V>
+__device__ __forceinline__ void st_n(T* p, const T* w) {
+    if constexpr (V * sizeof(T) == 16) {
+        stv(p, w);
+    } else {
+        static_assert(V == 2 && sizeof(T) == 4, "8-byte groups are float pairs");
+        *reinterpret_cast<float2*>(p) = make_float2(w[0], w[1]);
+    }
 }
 
-template <typename T, int NB>
-__device__ __forceinline__ void zero(T (&acc)[4][NB]) {
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < NB; ++b) acc[a][b] = T(0);
-}
+// ---------------------------------------------------------------------------
+// Accumulators. C (rows < nrows, KT columns) += A B, with A either row-major
+// (rows(): A[i*lda + k]) or transposed (cols(): A[k*lda + i]) and B row-major
+// (Bm[k*ldb + c]). visit(nrows, f) hands each thread's results to
+// f(row, col, T* v), v holding V adjacent columns.
+// ---------------------------------------------------------------------------
 
-// acc[a][b] += sum_{j<depth} A[(ty+16a)*lda + j] * Bm[j*ldb + col_of(tx,b)], a < NA
-template <typename T, int NB, int NA>
-__device__ __forceinline__ void mma_rows_n(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
-                                           int ty, int tx) {
-    constexpr int G = vec<T>();
-    const T* ap = A + ty * lda;
-    const T* bp = Bm + G * tx;
-    for (int j = 0; j < depth; ++j) {
-        T w[NB];
+// FP32 register tiles: thread (ty, tx) owns rows ty + 16a and 16-byte column
+// groups at vec*tx + 16*vec*h.
+template <typename T, int KT>
+struct AccScalar {
+    static constexpr int NB = KT / 16, G = vec<T>(), V = G;
+    T c[4][NB];
+
+    __device__ __forceinline__ void zero() {
 #pragma unroll
-        for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int a = 0; a < NA; ++a) {
-            const T l = ap[16 * a * lda + j];
+            for (int b = 0; b < NB; ++b) c[a][b] = T(0);
+    }
+
+    template <int NA>
+    __device__ __forceinline__ void rows_n(const T* A, int lda, const T* Bm, int ldb, int depth) {
+        const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+        const T* ap = A + ty * lda;
+        const T* bp = Bm + G * tx;
+        for (int j = 0; j < depth; ++j) {
+            T w[NB];
 #pragma unroll
-            for (int b = 0; b < NB; ++b) acc[a][b] += l * w[b];
+            for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                const T l = ap[16 * a * lda + j];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) c[a][b] += l * w[b];
+            }
         }
     }
-}
 
-// acc[a][b] += sum_{j<depth} A[j*lda + ty+16a] * Bm[j*ldb + col_of(tx,b)], a < NA   (A transposed)
-template <typename T, int NB, int NA>
-__device__ __forceinline__ void mma_cols_n(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
-                                           int ty, int tx) {
-    constexpr int G = vec<T>();
-    const T* bp = Bm + G * tx;
-    for (int j = 0; j < depth; ++j) {
-        T w[NB], l[NA];
+    template <int NA>
+    __device__ __forceinline__ void cols_n(const T* A, int lda, const T* Bm, int ldb, int depth) {
+        const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+        const T* bp = Bm + G * tx;
+        for (int j = 0; j < depth; ++j) {
+            T w[NB], l[NA];
 #pragma unroll
-        for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
+            for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
 #pragma unroll
-        for (int a = 0; a < NA; ++a) l[a] = A[j * lda + ty + 16 * a];
+            for (int a = 0; a < NA; ++a) l[a] = A[j * lda + ty + 16 * a];
 #pragma unroll
-        for (int a = 0; a < NA; ++a)
+            for (int a = 0; a < NA; ++a)
 #pragma unroll
-            for (int b = 0; b < NB; ++b) acc[a][b] += l[a] * w[b];
+                for (int b = 0; b < NB; ++b) c[a][b] += l[a] * w[b];
+        }
+    }
+
+    // only the 16-row blocks holding one of the first nrows rows are computed
+    __device__ __forceinline__ void rows(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
+        switch ((nrows + 15) >> 4) {
+            case 0: break;
+            case 1: rows_n<1>(A, lda, Bm, ldb, depth); break;
+            case 2: rows_n<2>(A, lda, Bm, ldb, depth); break;
+            case 3: rows_n<3>(A, lda, Bm, ldb, depth); break;
+            default: rows_n<4>(A, lda, Bm, ldb, depth); break;
+        }
+    }
+    __device__ __forceinline__ void cols(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
+        switch ((nrows + 15) >> 4) {
+            case 0: break;
+            case 1: cols_n<1>(A, lda, Bm, ldb, depth); break;
+            case 2: cols_n<2>(A, lda, Bm, ldb, depth); break;
+            case 3: cols_n<3>(A, lda, Bm, ldb, depth); break;
+            default: cols_n<4>(A, lda, Bm, ldb, depth); break;
+        }
+    }
+
+    template <class F>
+    __device__ __forceinline__ void visit(int nrows, F&& f) {
+        const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int t = ty + 16 * a;
+            if (t < nrows)
+#pragma unroll
+                for (int h = 0; h < NB / G; ++h) f(t, G * tx + 16 * G * h, &c[a][G * h]);
+        }
+    }
+};
+
+// FP64 tensor tiles (KT = 64): warp w owns columns [8w, 8w+8) and the 8-row
+// m8n8k4 tiles down to row 64; lane (g = lane/4, t = lane%4) holds rows 8m+g,
+// columns 8w+2t and 8w+2t+1. The depth must be a multiple of 4 with the padded
+// depths zero in both operands.
+struct AccDmma {
+    static constexpr int V = 2;
+    double c[8][2];
+
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int m = 0; m < 8; ++m) c[m][0] = c[m][1] = 0.0;
+    }
+
+    static __device__ __forceinline__ void mma(double (&d)[2], double a, double b) {
+        asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+            : "+d"(d[0]), "+d"(d[1])
+            : "d"(a), "d"(b));
+    }
+
+    template <int MT, bool TRANS>
+    __device__ __forceinline__ void run(const double* A, int lda, const double* Bm, int ldb, int depth) {
+        const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, n0 = 8 * (threadIdx.x >> 5);
+        const double* bp = Bm + t * ldb + n0 + g;
+        for (int k = 0; k < depth; k += 4) {
+            const double b = bp[k * ldb];
+#pragma unroll
+            for (int m = 0; m < MT; ++m) {
+                const double a = TRANS ? A[(k + t) * lda + 8 * m + g] : A[(8 * m + g) * lda + k + t];
+                mma(c[m], a, b);
+            }
+        }
+    }
+
+    template <bool TRANS>
+    __device__ __forceinline__ void dispatch(const double* A, int lda, const double* Bm, int ldb, int depth,
+                                             int nrows) {
+        switch ((nrows + 7) >> 3) {
+            case 0: break;
+            case 1: run<1, TRANS>(A, lda, Bm, ldb, depth); break;
+            case 2: run<2, TRANS>(A, lda, Bm, ldb, depth); break;
+            case 3: run<3, TRANS>(A, lda, Bm, ldb, depth); break;
+            case 4: run<4, TRANS>(A, lda, Bm, ldb, depth); break;
+            case 5: run<5, TRANS>(A, lda, Bm, ldb, depth); break;
+            case 6: run<6, TRANS>(A, lda, Bm, ldb, depth); break;
+            case 7: run<7, TRANS>(A, lda, Bm, ldb, depth); break;
+            default: run<8, TRANS>(A, lda, Bm, ldb, depth); break;
+        }
+    }
+    __device__ __forceinline__ void rows(const double* A, int lda, const double* Bm, int ldb, int depth,
+                                         int nrows) {
+        dispatch<false>(A, lda, Bm, ldb, depth, nrows);
+    }
+    __device__ __forceinline__ void cols(const double* A, int lda, const double* Bm, int ldb, int depth,
+                                         int nrows) {
+        dispatch<true>(A, lda, Bm, ldb, depth, nrows);
+    }
+
+    template <class F>
+    __device__ __forceinline__ void visit(int nrows, F&& f) {
+        const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, n0 = 8 * (threadIdx.x >> 5);
+#pragma unroll
+        for (int m = 0; m < 8; ++m)
+            if (8 * m + g < nrows) f(8 * m + g, n0 + 2 * t, c[m]);
+    }
+};
+
+template <typename T, int KT>
+struct AccSel {
+    using type = AccScalar<T, KT>;
+};
+template <>
+struct AccSel<double, 64> {
+    using type = AccDmma;
+};
+template <typename T, int KT>
+using Acc = typename AccSel<T, KT>::type;
+
+// Zero rows [r0, r1) x columns [0, ncols) of a shared tile (padding of a product's depth).
+template <typename T>
+__device__ __forceinline__ void zero_rows(T* D, int ld, int r0, int r1, int ncols) {
+    for (int e = threadIdx.x; e < (r1 - r0) * ncols; e += NT) {
+        const int r = e / ncols, c = e - r * ncols;
+        D[(r0 + r) * ld + c] = T(0);
     }
 }
-
-// Only the 16-row blocks that hold one of the first `nrows` rows are computed.
-template <typename T, int NB>
-__device__ __forceinline__ void mma_rows(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
-                                         int nrows, int ty, int tx) {
-    switch ((nrows + 15) >> 4) {
-        case 0: break;
-        case 1: mma_rows_n<T, NB, 1>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-        case 2: mma_rows_n<T, NB, 2>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-        case 3: mma_rows_n<T, NB, 3>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-        default: mma_rows_n<T, NB, 4>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-    }
-}
-
-template <typename T, int NB>
-__device__ __forceinline__ void mma_cols(T (&acc)[4][NB], const T* A, int lda, const T* Bm, int ldb, int depth,
-                                         int nrows, int ty, int tx) {
-    switch ((nrows + 15) >> 4) {
-        case 0: break;
-        case 1: mma_cols_n<T, NB, 1>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-        case 2: mma_cols_n<T, NB, 2>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-        case 3: mma_cols_n<T, NB, 3>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-        default: mma_cols_n<T, NB, 4>(acc, A, lda, Bm, ldb, depth, ty, tx); break;
-    }
-}
-
-// Rows ty+16a < nrows of acc into the row-major tile D (leading dimension ld).
-template <typename T, int NB>
-__device__ __forceinline__ void store_rows(T* D, int64_t ld, const T (&acc)[4][NB], int nrows, int ty, int tx) {
-    constexpr int G = vec<T>();
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int t = ty + 16 * a;
-        if (t < nrows)
-#pragma unroll
-            for (int h = 0; h < NB / G; ++h) stv(D + t * ld + G * tx + 16 * G * h, &acc[a][G * h]);
+// Zero columns [c0, c1) of rows [0, nrows).
+template <typename T>
+__device__ __forceinline__ void zero_cols(T* D, int ld, int nrows, int c0, int c1) {
+    const int w = c1 - c0;
+    for (int e = threadIdx.x; e < nrows * w; e += NT) {
+        const int r = e / w, c = e - r * w;
+        D[r * ld + c0 + c] = T(0);
     }
 }
 
@@ -185,14 +312,15 @@ __device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.com
 __device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void copy_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// Rows [0, nrows) of a KT-wide shared tile to an n x K array (g = first row, first column).
+// Rows [0, nrows) of a KT-wide shared tile (row stride ld) to an n x K array
+// (g = first row, first column).
 template <typename T, int KT>
-__device__ __forceinline__ void tile_rows_to_global(T* g, int64_t K, const T* D, int nrows) {
+__device__ __forceinline__ void tile_rows_to_global(T* g, int64_t K, const T* D, int ld, int nrows) {
     constexpr int VPR = KT / vec<T>();
     for (int i = threadIdx.x; i < nrows * VPR; i += NT) {
         const int r = i / VPR, v = i - r * VPR;
         *reinterpret_cast<uint4*>(g + r * K + v * vec<T>()) =
-            *reinterpret_cast<const uint4*>(D + r * KT + v * vec<T>());
+            *reinterpret_cast<const uint4*>(D + r * ld + v * vec<T>());
     }
 }
 
@@ -231,30 +359,30 @@ __device__ __forceinline__ void gather_issue(const SolveArgs<T>& a, const Gather
 
 // D rows (+ or -)= the staged entries [e0, e1) that belong to them, in entry order.
 template <typename T, int KT, bool SUB>
-__device__ __forceinline__ void gather_accumulate(T* D, const T* St, const unsigned char* live, const int* grs,
-                                                  int nrows, int e0, int e1) {
+__device__ __forceinline__ void gather_accumulate(T* D, int ld, const T* St, const unsigned char* live,
+                                                  const int* grs, int nrows, int e0, int e1) {
     constexpr int G = vec<T>(), TPR = KT / G, RG = NT / TPR;  // threads per row (one vector each), rows in parallel
     const int c = G * (threadIdx.x % TPR);
     for (int r = threadIdx.x / TPR; r < nrows; r += RG) {
         const int lo = max(grs[r], e0), hi = min(grs[r + 1], e1);
         if (lo >= hi) continue;
         T v[G], u[G];
-        ldv(D + r * KT + c, v);
+        ldv(D + r * ld + c, v);
         for (int e = lo; e < hi; ++e) {
             if (!live[e - e0]) continue;
             ldv(St + (e - e0) * KT + c, u);
 #pragma unroll
             for (int q = 0; q < G; ++q) v[q] = SUB ? v[q] - u[q] : v[q] + u[q];
         }
-        stv(D + r * KT + c, v);
+        stv(D + r * ld + c, v);
     }
 }
 
 // Waits for every copy this CTA has in flight (the caller has issued the
 // range's first chunk), then adds the range chunk by chunk.
 template <typename T, int KT, bool SUB>
-__device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const GatherRange& g, int k0, T* D, int nrows,
-                                              T* St, unsigned char* live, const int* grs) {
+__device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const GatherRange& g, int k0, T* D, int ld,
+                                              int nrows, T* St, unsigned char* live, const int* grs) {
     constexpr int SG = stage_rows<T>();
     int e0 = 0;
     do {
@@ -264,7 +392,7 @@ __device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const Gathe
         }
         copy_async_wait();
         __syncthreads();
-        if (g.E > 0) gather_accumulate<T, KT, SUB>(D, St, live, grs, nrows, e0, min(g.E, e0 + SG));
+        if (g.E > 0) gather_accumulate<T, KT, SUB>(D, ld, St, live, grs, nrows, e0, min(g.E, e0 + SG));
         __syncthreads();
         e0 += SG;
     } while (e0 < g.E);
@@ -272,11 +400,11 @@ __device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const Gathe
 
 template <typename T, int KT>
 __global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
-    constexpr int NB = KT / 16, VPR = KT / vec<T>();
+    constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_fwd_a<T>(), DP = depth_pad<T>();
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* Wt = reinterpret_cast<T*>(smraw);   // TR x KT: W, then X, then this chunk's update rows
-    T* Lp = Wt + TR * KT;                   // TR x LDP: inverse diagonal block, then the panel chunk
-    T* St = Lp + TR * LDP;                  // stage_rows x KT: children's update rows
+    T* Wt = reinterpret_cast<T*>(smraw);   // TR x LW: W, then X, then this chunk's update rows
+    T* Lp = Wt + TR * LW;                   // TR x LA: inverse diagonal block, then the panel chunk
+    T* St = Lp + TR * LA;                   // stage_rows x KT: children's update rows
     __shared__ int grs[TR + 1];
     __shared__ unsigned char live[stage_rows<T>()];
     const int2 task = a.tasks[t0 + blockIdx.x];
@@ -284,9 +412,9 @@ __global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
     if (a.reach && !a.reach[s]) return;
     const DevPlan& p = a.p;
     const int tid = threadIdx.x;
-    const int ty = tid >> 4, tx = tid & 15;
     const int K = a.K, k0 = blockIdx.y * KT;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, m = p.sn_m[s], nr = m - ns;
+    const int nsp = (ns + DP - 1) / DP * DP;  // product depth
     const int64_t fb = p.sn_rowptr[s];
     const int q0 = chunk * TR;
     const int nq = nr > 0 ? min(TR, nr - q0) : 0;
@@ -296,32 +424,36 @@ __global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
     const T* inv = a.inv + p.sn_invptr[s];
     for (int e = tid; e < ns * ns; e += NT) {
         const int i = e / ns, j = e - i * ns;
-        copy_async(&Lp[i * LDP + j], inv + e);
+        copy_async(&Lp[i * LA + j], inv + e);
     }
     if (a.delta_src) {
         for (int e = tid; e < ns * KT; e += NT) {
             const int f = e / KT, c = e - f * KT;
-            Wt[f * KT + c] = (a.delta_src[k0 + c] == c0 + f) ? T(1) : T(0);
+            Wt[f * LW + c] = (a.delta_src[k0 + c] == c0 + f) ? T(1) : T(0);
         }
     } else {
         for (int i = tid; i < ns * VPR; i += NT) {
             const int f = i / VPR, v = i - f * VPR;
-            copy16_async(Wt + f * KT + v * vec<T>(), a.R + (int64_t)(c0 + f) * K + k0 + v * vec<T>());
+            copy16_async(Wt + f * LW + v * vec<T>(), a.R + (int64_t)(c0 + f) * K + k0 + v * vec<T>());
         }
+    }
+    if (nsp > ns) {  // padded depth: zero in both operands (also for X below)
+        zero_rows(Wt, LW, ns, nsp, KT);
+        zero_cols(Lp, LA, ns, ns, nsp);
     }
     const GatherRange g1 = gather_open(a, fb, 0, ns, grs);
     if (g1.E > 0) gather_issue<T, KT>(a, g1, 0, k0, St, live);
     copy_async_commit();
-    gather_finish<T, KT, true>(a, g1, k0, Wt, ns, St, live, grs);
+    gather_finish<T, KT, true>(a, g1, k0, Wt, LW, ns, St, live, grs);
 
     // X = inv(L_ss) W, written over W
-    T acc[4][NB];
-    zero(acc);
-    mma_rows(acc, Lp, LDP, Wt, KT, ns, ns, ty, tx);
+    Acc<T, KT> acc;
+    acc.zero();
+    acc.rows(Lp, LA, Wt, LW, nsp, ns);
     __syncthreads();
-    store_rows(Wt, KT, acc, ns, ty, tx);
+    acc.visit(ns, [&](int r, int c, T* v) { st_n<T, Acc<T, KT>::V>(Wt + r * LW + c, v); });
     __syncthreads();
-    if (chunk == 0) tile_rows_to_global<T, KT>(a.B + (int64_t)c0 * K + k0, K, Wt, ns);
+    if (chunk == 0) tile_rows_to_global<T, KT>(a.B + (int64_t)c0 * K + k0, K, Wt, LW, ns);
     if (nq <= 0) return;
 
     // U_s rows of this chunk = L_rs X + the children's rows landing on them; the
@@ -329,38 +461,40 @@ __global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
     const T* P = a.val + p.sn_valptr[s] + (int64_t)(ns + q0) * ns;
     for (int e = tid; e < nq * ns; e += NT) {
         const int r = e / ns, j = e - r * ns;
-        copy_async(&Lp[r * LDP + j], P + e);
+        copy_async(&Lp[r * LA + j], P + e);
     }
+    if (nsp > ns) zero_cols(Lp, LA, nq, ns, nsp);
     const GatherRange g2 = gather_open(a, fb, ns + q0, nq, grs);
     if (g2.E > 0) gather_issue<T, KT>(a, g2, 0, k0, St, live);
     copy_async_commit();
     copy_async_wait();
     __syncthreads();
-    zero(acc);
-    mma_rows(acc, Lp, LDP, Wt, KT, ns, nq, ty, tx);
+    acc.zero();
+    acc.rows(Lp, LA, Wt, LW, nsp, nq);
     __syncthreads();
-    store_rows(Wt, KT, acc, nq, ty, tx);
-    gather_finish<T, KT, false>(a, g2, k0, Wt, nq, St, live, grs);
-    tile_rows_to_global<T, KT>(a.U + (a.uoff[s] + q0) * (int64_t)K + k0, K, Wt, nq);
+    acc.visit(nq, [&](int r, int c, T* v) { st_n<T, Acc<T, KT>::V>(Wt + r * LW + c, v); });
+    gather_finish<T, KT, false>(a, g2, k0, Wt, LW, nq, St, live, grs);
+    tile_rows_to_global<T, KT>(a.U + (a.uoff[s] + q0) * (int64_t)K + k0, K, Wt, LW, nq);
 }
 
 template <typename T, int KT>
 __global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
-    constexpr int NB = KT / 16, VPR = KT / vec<T>(), G = vec<T>();
-    constexpr int PS = RC * TR, XS = RC * KT;  // one chunk buffer: panel rows, gathered solution rows
-    static_assert(2 * (PS + XS) >= TR * KT + TR * TR, "the finishing tiles alias the chunk buffers");
+    constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_bwd_a<T>(), DP = depth_pad<T>();
+    constexpr int PS = RC * LA, XS = RC * LW;  // one chunk buffer: panel rows, gathered solution rows
+    static_assert(2 * (PS + XS) >= TR * LW + TR * LA, "the finishing tiles alias the chunk buffers");
+    using AccT = Acc<T, KT>;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* buf = reinterpret_cast<T*>(smraw);
-    T* Cs = buf;             // TR x KT, after the gather
-    T* Ms = buf + TR * KT;   // TR x TR inverse diagonal block, after the gather
+    T* Cs = buf;             // TR x LW, after the gather
+    T* Ms = buf + TR * LW;   // TR x LA inverse diagonal block, after the gather
     __shared__ int last_arrival;
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, split = task.y;
     const DevPlan& p = a.p;
     const int tid = threadIdx.x;
-    const int ty = tid >> 4, tx = tid & 15;
     const int K = a.K, k0 = blockIdx.y * KT;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, m = p.sn_m[s], nr = m - ns;
+    const int nsp = (ns + DP - 1) / DP * DP;
     const int nspl = a.nsplit[s];
     const int q0 = split * kSplitRows, q1 = min(nr, q0 + kSplitRows);
     const T* P = a.val + p.sn_valptr[s];
@@ -368,21 +502,25 @@ __global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
 
     // chunk ci of the split's structure rows into buffer ci & 1
     auto issue = [&](int ci) {
-        const int qq = q0 + ci * RC, nc = min(RC, q1 - qq);
+        const int qq = q0 + ci * RC, nc = min(RC, q1 - qq), ncp = (nc + DP - 1) / DP * DP;
         T* Ps = buf + (ci & 1) * (PS + XS);
         T* Xg = Ps + PS;
         for (int e = tid; e < nc * ns; e += NT) {
             const int r = e / ns, j = e - r * ns;
-            copy_async(&Ps[r * TR + j], P + (int64_t)(ns + qq + r) * ns + j);
+            copy_async(&Ps[r * LA + j], P + (int64_t)(ns + qq + r) * ns + j);
         }
         for (int i = tid; i < nc * VPR; i += NT) {
             const int r = i / VPR, v = i - r * VPR;
-            copy16_async(Xg + r * KT + v * vec<T>(), a.B + (int64_t)rows[ns + qq + r] * K + k0 + v * vec<T>());
+            copy16_async(Xg + r * LW + v * vec<T>(), a.B + (int64_t)rows[ns + qq + r] * K + k0 + v * vec<T>());
+        }
+        if (ncp > nc) {
+            zero_rows(Ps, LA, nc, ncp, TR);
+            zero_rows(Xg, LW, nc, ncp, KT);
         }
         copy_async_commit();
     };
-    T acc[4][NB];
-    zero(acc);
+    AccT acc;
+    acc.zero();
     const int nchunks = q1 > q0 ? (q1 - q0 + RC - 1) / RC : 0;
     if (nchunks > 0) issue(0);
     for (int ci = 0; ci < nchunks; ++ci) {
@@ -394,14 +532,16 @@ __global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
         }
         __syncthreads();
         const T* Ps = buf + (ci & 1) * (PS + XS);
-        mma_cols(acc, Ps, TR, Ps + PS, KT, min(RC, q1 - q0 - ci * RC), ns, ty, tx);
+        const int nc = min(RC, q1 - q0 - ci * RC);
+        acc.cols(Ps, LA, Ps + PS, LW, (nc + DP - 1) / DP * DP, ns);
         __syncthreads();
     }
 
     const bool zero_y = a.reach && !a.reach[s];
     if (nspl > 1) {
         T* part = a.part + a.poff[s] * (int64_t)TR * K + k0;
-        store_rows(part + (int64_t)split * TR * K, (int64_t)K, acc, ns, ty, tx);
+        T* mine = part + (int64_t)split * TR * K;
+        acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(mine + (int64_t)r * K + c, v); });
         __threadfence();
         __syncthreads();
         if (tid == 0) {
@@ -411,47 +551,42 @@ __global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
         __syncthreads();
         if (!last_arrival) return;
         __threadfence();
+        acc.visit(ns, [&](int r, int c, T* v) {
 #pragma unroll
-        for (int aa = 0; aa < 4; ++aa) {
-            const int t = ty + 16 * aa;
-            if (t < ns)
-#pragma unroll
-                for (int b = 0; b < NB; ++b) {
-                    T sum = T(0);
-                    for (int sp = 0; sp < nspl; ++sp)
-                        sum += __ldcg(&part[((int64_t)sp * TR + t) * K + col_of<T>(tx, b)]);
-                    acc[aa][b] = sum;
-                }
-        }
+            for (int q = 0; q < AccT::V; ++q) {
+                T sum = T(0);
+                for (int sp = 0; sp < nspl; ++sp) sum += __ldcg(&part[((int64_t)sp * TR + r) * K + c + q]);
+                v[q] = sum;
+            }
+        });
         if (tid == 0) a.counters[(int64_t)s * a.ktiles + blockIdx.y] = 0;
     }
     // C = y - acc; X_s = inv(L_ss)^T C
     const T* inv = a.inv + p.sn_invptr[s];
     for (int e = tid; e < ns * ns; e += NT) {
         const int i = e / ns, j = e - i * ns;
-        copy_async(&Ms[i * TR + j], inv + e);
+        copy_async(&Ms[i * LA + j], inv + e);
     }
     copy_async_commit();
-#pragma unroll
-    for (int aa = 0; aa < 4; ++aa) {
-        const int t = ty + 16 * aa;
-        if (t < ns)
-#pragma unroll
-            for (int h = 0; h < NB / G; ++h) {
-                T y[G];
-#pragma unroll
-                for (int q = 0; q < G; ++q) y[q] = T(0);
-                if (!zero_y) ldv(a.B + (int64_t)(c0 + t) * K + k0 + G * tx + 16 * G * h, y);
-#pragma unroll
-                for (int q = 0; q < G; ++q) y[q] -= acc[aa][G * h + q];
-                stv(Cs + t * KT + G * tx + 16 * G * h, y);
-            }
+    if (nsp > ns) {
+        zero_rows(Ms, LA, ns, nsp, TR);
+        zero_rows(Cs, LW, ns, nsp, KT);
     }
+    acc.visit(ns, [&](int r, int c, T* v) {
+        T y[AccT::V];
+#pragma unroll
+        for (int q = 0; q < AccT::V; ++q) y[q] = T(0);
+        if (!zero_y) ld_n<T, AccT::V>(a.B + (int64_t)(c0 + r) * K + k0 + c, y);
+#pragma unroll
+        for (int q = 0; q < AccT::V; ++q) y[q] -= v[q];
+        st_n<T, AccT::V>(Cs + r * LW + c, y);
+    });
     copy_async_wait();
     __syncthreads();
-    zero(acc);
-    mma_cols(acc, Ms, TR, Cs, KT, ns, ns, ty, tx);
-    store_rows(a.B + (int64_t)c0 * K + k0, (int64_t)K, acc, ns, ty, tx);
+    acc.zero();
+    acc.cols(Ms, LA, Cs, LW, nsp, ns);
+    T* out = a.B + (int64_t)c0 * K + k0;
+    acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(out + (int64_t)r * K + c, v); });
 }
 
 __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __restrict__ parent,
@@ -469,9 +604,13 @@ __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __res
 }
 
 template <typename T, int KT>
-constexpr size_t fwd_smem() { return (size_t)(TR * KT + TR * LDP + stage_rows<T>() * KT) * sizeof(T); }
+constexpr size_t fwd_smem() {
+    return (size_t)(TR * ld_rows<T, KT>() + TR * ld_fwd_a<T>() + stage_rows<T>() * KT) * sizeof(T);
+}
 template <typename T, int KT>
-constexpr size_t bwd_smem() { return (size_t)2 * (RC * TR + RC * KT) * sizeof(T); }
+constexpr size_t bwd_smem() {
+    return (size_t)2 * (RC * ld_bwd_a<T>() + RC * ld_rows<T, KT>()) * sizeof(T);
+}
 
 template <typename T, int KT>
 cudaError_t set_smem() {
