@@ -80,7 +80,7 @@ struct Workspace {
     float* dT32 = nullptr;
     int32_t* src = nullptr;
     uint8_t* reach = nullptr;
-    int32_t* band = nullptr;
+    int4* band = nullptr;
     int32_t* longf = nullptr;
     double* out = nullptr;
     int32_t out_stride = 0;
@@ -123,6 +123,9 @@ struct fcw_engine {
     double *coords_d = nullptr, *varea_d = nullptr, *farea_d = nullptr, *g11_d = nullptr, *g12_d = nullptr,
            *g22_d = nullptr;
     int32_t* boundary_d = nullptr;
+    int4* inc_rec_d = nullptr;        // per incidence: face, corners (elimination order)
+    long long* farea_fx_d = nullptr;  // lean face areas in fixed point
+    double area_unscale = 0.0;
     int* err_d = nullptr;
     std::vector<Workspace> pool;  // blocks in flight: workspace i runs on pool[i].stream
     size_t cur_ws = 0;
@@ -444,6 +447,23 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
                 fill[v]++;
             }
     }
+    // the same incidences as records holding the face's corners, and the face areas
+    // in a fixed point whose full scale is 2^62 >= the total, so that per-bin
+    // sums are exact and independent of the order atomics add them in
+    std::vector<int4> inc_rec(3 * nf);
+    for (int64_t q = 0; q < 3 * nf; ++q) {
+        const int32_t f = inc_face[q];
+        inc_rec[q] = make_int4(f, fv[3 * f], fv[3 * f + 1], fv[3 * f + 2]);
+    }
+    double lean_sum = 0.0;
+    for (double x : m.lean_area) lean_sum += x;
+    const int area_exp = lean_sum > 0.0 ? (int)std::ceil(std::log2(lean_sum)) : 0;
+    const double area_scale = std::ldexp(1.0, 62 - area_exp);
+    std::vector<long long> farea_fx(nf);
+    for (int64_t f = 0; f < nf; ++f) farea_fx[f] = std::llround(m.lean_area[f] * area_scale);
+    e->area_unscale = 1.0 / area_scale;
+    FCW_TRY(e->upload(&e->inc_rec_d, inc_rec));
+    FCW_TRY(e->upload(&e->farea_fx_d, farea_fx));
     int32_t *fv_d, *inc_ptr_d, *inc_face_d;
     int8_t* inc_corner_d;
     double *gb_d, *garea_d;
@@ -665,6 +685,9 @@ int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, do
     a.inc_ptr = e->fd.inc_ptr;
     a.inc_face = e->fd.inc_face;
     a.inc_corner = e->fd.inc_corner;
+    a.inc_rec = e->inc_rec_d;
+    a.farea_fx = e->farea_fx_d;
+    a.area_unscale = e->area_unscale;
     a.total_area = e->lean_total;
     a.farea = e->farea_d;
     a.g11 = e->g11_d;
@@ -1150,7 +1173,8 @@ extern "C" int fcw_field_metrics_static(fcw_engine* e, const double* d_dev, cons
                         + align256((size_t)ntiles * K * 8 * sizeof(double))  // health/MSD partials
                         + align256((size_t)n * K * sizeof(int32_t))       // near-vertex lists
                         + align256((size_t)K * sizeof(int32_t))           // near-vertex counts
-                        + 2 * align256((size_t)nf * K * sizeof(int32_t))  // near faces by bin, long faces
+                        + align256((size_t)nf * K * sizeof(int4))         // near faces by bin
+                        + align256((size_t)nf * K * sizeof(int32_t))      // long faces
                         + align256((size_t)K * sizeof(int32_t));          // sources (elimination order)
     if (need > kStaticScratchBytes)
         return fail(FCW_E_INVALID, "mesh too large for fcw_field_metrics_static: needs " + std::to_string(need) +
@@ -1169,7 +1193,7 @@ extern "C" int fcw_field_metrics_static(fcw_engine* e, const double* d_dev, cons
     double* partials = reinterpret_cast<double*>(take((size_t)ntiles * K * 8 * sizeof(double)));
     int32_t* near_list = reinterpret_cast<int32_t*>(take((size_t)n * K * sizeof(int32_t)));
     int32_t* near_count = reinterpret_cast<int32_t*>(take((size_t)K * sizeof(int32_t)));
-    int32_t* band = reinterpret_cast<int32_t*>(take((size_t)nf * K * sizeof(int32_t)));
+    int4* band = reinterpret_cast<int4*>(take((size_t)nf * K * sizeof(int4)));
     int32_t* longf = reinterpret_cast<int32_t*>(take((size_t)nf * K * sizeof(int32_t)));
     int32_t* src = reinterpret_cast<int32_t*>(take((size_t)K * sizeof(int32_t)));
 

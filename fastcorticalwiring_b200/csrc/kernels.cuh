@@ -120,6 +120,9 @@ struct MetricArgs {
     const int32_t* inc_ptr = nullptr;   // vertex -> incident faces (elimination order)
     const int32_t* inc_face = nullptr;
     const int8_t* inc_corner = nullptr;
+    const int4* inc_rec = nullptr;      // per incidence (inc_face order): face, its three corners
+    const long long* farea_fx = nullptr;  // lean face areas in fixed point (exact order-free sums)
+    double area_unscale = 0.0;          // fixed point -> area
     double total_area = 0.0;            // sum of the lean face areas
     const double* farea = nullptr;      // lean face area, g11, g12, g22 (lean_geometry.py:44-63)
     const double* g11 = nullptr;
@@ -130,7 +133,7 @@ struct MetricArgs {
     double targets[kMaxTargets];
     double fracs[kMaxBetween];
     const int32_t* src = nullptr;       // elimination-order source per column
-    int32_t* band = nullptr;            // nsrc * nf scratch: near faces sorted by bin
+    int4* band = nullptr;               // nsrc * nf scratch: near faces (face, corners) sorted by bin
     int32_t* longf = nullptr;           // nsrc * nf scratch: near long faces
     double* out = nullptr;              // nsrc * stride
     int* err = nullptr;

@@ -197,7 +197,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 struct SrcShared {
-    double pre[kMaxBins + 1];  // vertex-area histogram (fixed point) first, then face-area prefix sums
+    union {
+        unsigned long long hist[kMaxBins + 1];  // face areas per bin, fixed point (order-free sums)
+        double pre[kMaxBins + 1];               // then the exclusive prefix sums of the bins' areas
+    };
     int ptr[kMaxBins + 1];     // faces per bin -> exclusive prefix
     int fill[kMaxBins];
     double red[16][4];
@@ -214,7 +217,7 @@ struct Field {
     const T* d;
     const MetricArgs* a;
     SrcShared* s;
-    const int32_t* band;   // near faces sorted by bin
+    const int4* band;      // near faces (face, corners) sorted by bin
     const int32_t* longf;  // near faces whose distance extent exceeds the bin width
 
     __device__ double dv(int v) const { return (double)d[v]; }
@@ -237,13 +240,39 @@ struct Field {
         }
     }
 
+    // face_term of a band record (face, corners): no lookup of the face's corners
+    __device__ void rec_term(const int4& q, double d0, double d1, double d2, double r, int mode, double& x1,
+                             double& x2) const {
+        double ar, da;
+        face_cdf(d0, d1, d2, a->farea[q.x], r, ar, da);
+        if (mode == 0) {
+            x1 += ar;
+            x2 += da;
+        } else if (da > 0.0) {
+            x1 += da * grad_norm(d0, d1, d2, a->g11[q.x], a->g12[q.x], a->g22[q.x]);
+        }
+    }
+
     // Faces with bin in [kr, kend) plus long faces with bin >= kend, summed by one warp.
     __device__ void band_sum(int kr, int kend, double r, int mode, double& s1, double& s2) const {
         const int lane = threadIdx.x & 31;
         double x1 = 0.0, x2 = 0.0;
         const int* fv = a->fv;
         if (kend <= s->rc) {
-            for (int j = s->ptr[kr] + lane; j < s->ptr[kend]; j += 32) face_term(band[j], r, mode, x1, x2);
+            // two records per lane in flight
+            int j = s->ptr[kr] + lane;
+            const int je = s->ptr[kend];
+            for (; j + 32 < je; j += 64) {
+                const int4 q0 = band[j], q1 = band[j + 32];
+                const double a0 = dv(q0.y), a1 = dv(q0.z), a2 = dv(q0.w);
+                const double b0 = dv(q1.y), b1 = dv(q1.z), b2 = dv(q1.w);
+                rec_term(q0, a0, a1, a2, r, mode, x1, x2);
+                rec_term(q1, b0, b1, b2, r, mode, x1, x2);
+            }
+            if (j < je) {
+                const int4 q0 = band[j];
+                rec_term(q0, dv(q0.y), dv(q0.z), dv(q0.w), r, mode, x1, x2);
+            }
         } else {  // beyond the complete bins: scan every face (not reached for healthy fields)
             for (int f = lane; f < a->nf; f += 32) {
                 const double d0 = dv(fv[3 * f]), d1 = dv(fv[3 * f + 1]), d2 = dv(fv[3 * f + 2]);
@@ -353,7 +382,7 @@ __global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* _
     double* o = a.out + (int64_t)k * a.stride;
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     const T* d = dT + (int64_t)k * a.n;
-    int32_t* band = a.band + (int64_t)k * a.nf;
+    int4* band = a.band + (int64_t)k * a.nf;
     int32_t* longf = a.longf + (int64_t)k * a.nf;
     const double w = a.width;
 
@@ -431,7 +460,7 @@ __global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* _
     for (int attempt = 0; attempt < 32; ++attempt) {
         const int rc = S.rc;
         for (int i = tid; i <= kMaxBins; i += bs) {
-            S.pre[i] = 0.0;
+            S.hist[i] = 0ull;
             S.ptr[i] = 0;
             if (i < kMaxBins) S.fill[i] = 0;
         }
@@ -448,10 +477,10 @@ __global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* _
                 const double di = (double)d[i];
                 if (!(di < R)) continue;
                 for (int q = a.inc_ptr[i]; q < a.inc_ptr[i + 1]; ++q) {
-                    const int f = a.inc_face[q];
+                    const int4 rec = a.inc_rec[q];
+                    const int f = rec.x;
                     const int c = a.inc_corner[q];
-                    const int v0 = a.fv[3 * f], v1 = a.fv[3 * f + 1], v2 = a.fv[3 * f + 2];
-                    const double d0 = (double)d[v0], d1 = (double)d[v1], d2 = (double)d[v2];
+                    const double d0 = (double)d[rec.y], d1 = (double)d[rec.z], d2 = (double)d[rec.w];
                     if (c >= 1 && d0 < R) continue;   // an earlier corner emits it
                     if (c == 2 && d1 < R) continue;
                     if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
@@ -464,11 +493,11 @@ __global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* _
                     if (pass == 0) {
                         if (hi - lo > w) longf[atomicAdd(&S.nlong, 1)] = f;
                         if (kb <= rc && kb < kMaxBins) {
-                            atomicAdd(&S.pre[kb], a.farea[f]);
+                            atomicAdd(&S.hist[kb], (unsigned long long)a.farea_fx[f]);
                             atomicAdd(&S.ptr[kb], 1);
                         }
                     } else if (kb <= rc && kb < kMaxBins) {
-                        band[S.ptr[kb] + atomicAdd(&S.fill[kb], 1)] = f;
+                        band[S.ptr[kb] + atomicAdd(&S.fill[kb], 1)] = rec;
                     }
                 }
             }
@@ -481,7 +510,7 @@ __global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* _
                     const int b0 = min(lane * chunk, nbb), b1 = min(b0 + chunk, nbb);
                     double sa = 0.0;
                     int sc = 0;
-                    for (int b = b0; b < b1; ++b) { sa += S.pre[b]; sc += S.ptr[b]; }
+                    for (int b = b0; b < b1; ++b) { sa += (double)S.hist[b] * a.area_unscale; sc += S.ptr[b]; }
                     double ea = sa;
                     int ec = sc;
                     for (int off = 1; off < 32; off <<= 1) {
@@ -492,7 +521,7 @@ __global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* _
                     double ra = ea - sa;
                     int rcn = ec - sc;
                     for (int b = b0; b < b1; ++b) {
-                        const double xa = S.pre[b];
+                        const double xa = (double)S.hist[b] * a.area_unscale;
                         const int xc = S.ptr[b];
                         S.pre[b] = ra;
                         S.ptr[b] = rcn;
