@@ -178,7 +178,7 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
  * the reference. Its scratch is one 64 MiB array compiled into the library
  * (held by every device that loads it until the process exits); it takes at most
  * 32 fields per call and rejects meshes whose scratch would not fit with
- * FCW_E_INVALID (roughly 40k vertices with 32 fields). It calls no allocator.
+ * FCW_E_INVALID (roughly 34k vertices with 32 fields). It calls no allocator.
  * The first call on each device looks up the array's device address; make that
  * call before any stream capture. Every call reuses the same array, so calls
  * that overlap on the GPU (other streams, other threads) race: serialise them. */
