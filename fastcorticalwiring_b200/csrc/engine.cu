@@ -464,6 +464,25 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     e->area_unscale = 1.0 / area_scale;
     FCW_TRY(e->upload(&e->inc_rec_d, inc_rec));
     FCW_TRY(e->upload(&e->farea_fx_d, farea_fx));
+    std::vector<int4> inc_corners(3 * nf);
+    std::vector<float4> inc_coef(3 * nf);
+    std::vector<float2> inc_w(3 * nf);
+    for (int64_t q = 0; q < 3 * nf; ++q) {
+        const int32_t f = inc_face[q];
+        const float c11 = coef[4 * f], c12 = coef[4 * f + 1], c22 = coef[4 * f + 2];
+        inc_corners[q] = make_int4(fv[3 * f], fv[3 * f + 1], fv[3 * f + 2], inc_corner[q]);
+        inc_coef[q] = make_float4(c11, c12, c22, coef[4 * f + 3]);
+        // the corner weights in FP32, as the kernel's form defines them
+        if (inc_corner[q] == 0) inc_w[q] = make_float2(-(c11 + c12), -(c12 + c22));
+        else if (inc_corner[q] == 1) inc_w[q] = make_float2(c11, c12);
+        else inc_w[q] = make_float2(c12, c22);
+    }
+    int4* inc_corners_d;
+    float4* inc_coef_d;
+    float2* inc_w_d;
+    FCW_TRY(e->upload(&inc_corners_d, inc_corners));
+    FCW_TRY(e->upload(&inc_coef_d, inc_coef));
+    FCW_TRY(e->upload(&inc_w_d, inc_w));
     int32_t *fv_d, *inc_ptr_d, *inc_face_d;
     int8_t* inc_corner_d;
     double *gb_d, *garea_d;
@@ -477,6 +496,7 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     FCW_TRY(e->upload(&inc_corner_d, inc_corner));
     e->fd.nv = (int32_t)n; e->fd.nf = (int32_t)nf; e->fd.fv = fv_d; e->fd.gb = gb_d; e->fd.garea = garea_d;
     e->fd.coef = coef_d; e->fd.inc_ptr = inc_ptr_d; e->fd.inc_face = inc_face_d; e->fd.inc_corner = inc_corner_d;
+    e->fd.inc_corners = inc_corners_d; e->fd.inc_coef = inc_coef_d; e->fd.inc_w = inc_w_d;
     FCW_TRY(e->upload(&e->coords_d, coords));
     FCW_TRY(e->upload(&e->varea_d, varea));
     FCW_TRY(e->upload(&e->boundary_d, bnd));

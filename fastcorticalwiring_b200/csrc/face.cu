@@ -60,36 +60,73 @@ __device__ __forceinline__ double unit_scale(double m) {
     return __longlong_as_double((long long)(1023 - e) << 52);
 }
 
+// Mixed form, 64*NP columns per warp: lane l owns the column pairs {2l, 2l+1} + 64p,
+// p < NP, of the warp's slice (one 16-byte load per pair and vertex row, 512
+// contiguous bytes across the warp). The vertex's incidence records are read
+// once, lane j holding the j-th, and broadcast face by face.
+template <int NP>
 __global__ void __launch_bounds__(256) k_div_mixed(FaceData fd, const double* __restrict__ u,
                                                    float* __restrict__ div, int32_t K, int32_t ground) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int v = blockIdx.x * 8 + warp;
     if (v >= fd.nv) return;
-    const int col = blockIdx.y * kSlice + lane;
-    float acc = 0.0f;
+    const int64_t c0 = (int64_t)blockIdx.y * 64 * NP + 2 * lane;
+    float acc[2 * NP];
+#pragma unroll
+    for (int t = 0; t < 2 * NP; ++t) acc[t] = 0.0f;
     if (v != ground) {
-        for (int q = fd.inc_ptr[v]; q < fd.inc_ptr[v + 1]; ++q) {
-            const int f = fd.inc_face[q];
-            const int c = fd.inc_corner[q];
-            const int i0 = fd.fv[3 * f], i1 = fd.fv[3 * f + 1], i2 = fd.fv[3 * f + 2];
-            const double u0 = u[(int64_t)i0 * K + col];
-            const double d1 = u[(int64_t)i1 * K + col] - u0;
-            const double d2 = u[(int64_t)i2 * K + col] - u0;
-            const double mx = fmax(fabs(d1), fabs(d2));
-            if (!(mx >= 2.2250738585072014e-308)) continue;  // zero (or subnormal) gradient
-            const double sc = unit_scale(mx);
-            const float a1 = (float)(d1 * sc), a2 = (float)(d2 * sc);
-            const float4 cf = reinterpret_cast<const float4*>(fd.coef)[f];  // c11, c12, c22, area
-            const float qn = a1 * a1 * cf.x + 2.0f * a1 * a2 * cf.y + a2 * a2 * cf.z;
-            if (!(qn > 0.0f)) continue;
-            float w1, w2;
-            if (c == 0) { w1 = -(cf.x + cf.y); w2 = -(cf.y + cf.z); }
-            else if (c == 1) { w1 = cf.x; w2 = cf.y; }
-            else { w1 = cf.y; w2 = cf.z; }
-            acc -= cf.w * (a1 * w1 + a2 * w2) * rsqrtf(qn);
+        const int q0 = fd.inc_ptr[v], deg = fd.inc_ptr[v + 1] - q0;
+        for (int jb = 0; jb < deg; jb += 32) {
+            const int nj = min(32, deg - jb);
+            int4 rv = make_int4(0, 0, 0, 0);
+            float4 rc = make_float4(0.f, 0.f, 0.f, 0.f);
+            float2 rw = make_float2(0.f, 0.f);
+            if (lane < nj) {
+                rv = fd.inc_corners[q0 + jb + lane];
+                rc = fd.inc_coef[q0 + jb + lane];
+                rw = fd.inc_w[q0 + jb + lane];
+            }
+            for (int j = 0; j < nj; ++j) {
+                const int i0 = __shfl_sync(0xffffffffu, rv.x, j);
+                const int i1 = __shfl_sync(0xffffffffu, rv.y, j);
+                const int i2 = __shfl_sync(0xffffffffu, rv.z, j);
+                const double* p0 = u + (int64_t)i0 * K + c0;
+                const double* p1 = u + (int64_t)i1 * K + c0;
+                const double* p2 = u + (int64_t)i2 * K + c0;
+                double u0[2 * NP], u1[2 * NP], u2[2 * NP];
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    const double2 x0 = *reinterpret_cast<const double2*>(p0 + 64 * q);
+                    const double2 x1 = *reinterpret_cast<const double2*>(p1 + 64 * q);
+                    const double2 x2 = *reinterpret_cast<const double2*>(p2 + 64 * q);
+                    u0[2 * q] = x0.x; u0[2 * q + 1] = x0.y;
+                    u1[2 * q] = x1.x; u1[2 * q + 1] = x1.y;
+                    u2[2 * q] = x2.x; u2[2 * q + 1] = x2.y;
+                }
+                const float c11 = __shfl_sync(0xffffffffu, rc.x, j);
+                const float c12 = __shfl_sync(0xffffffffu, rc.y, j);
+                const float c22 = __shfl_sync(0xffffffffu, rc.z, j);
+                const float area = __shfl_sync(0xffffffffu, rc.w, j);
+                const float w1 = __shfl_sync(0xffffffffu, rw.x, j);
+                const float w2 = __shfl_sync(0xffffffffu, rw.y, j);
+#pragma unroll
+                for (int t = 0; t < 2 * NP; ++t) {
+                    const double d1 = u1[t] - u0[t];
+                    const double d2 = u2[t] - u0[t];
+                    const double mx = fmax(fabs(d1), fabs(d2));
+                    if (!(mx >= 2.2250738585072014e-308)) continue;  // zero (or subnormal) gradient
+                    const double sc = unit_scale(mx);
+                    const float x1 = (float)(d1 * sc), x2 = (float)(d2 * sc);
+                    const float qn = x1 * x1 * c11 + 2.0f * x1 * x2 * c12 + x2 * x2 * c22;
+                    if (!(qn > 0.0f)) continue;
+                    acc[t] -= area * (x1 * w1 + x2 * w2) * rsqrtf(qn);
+                }
+            }
         }
     }
-    div[(int64_t)v * K + col] = acc;
+    float* o = div + (int64_t)v * K + c0;
+#pragma unroll
+    for (int q = 0; q < NP; ++q) *reinterpret_cast<float2*>(o + 64 * q) = make_float2(acc[2 * q], acc[2 * q + 1]);
 }
 
 }  // namespace
@@ -102,7 +139,10 @@ void launch_divergence_fp64(const FaceData& fd, const double* u, double* div, in
 void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,
                              cudaStream_t st) {
     if (fd.nv <= 0 || K <= 0) return;
-    k_div_mixed<<<dim3((fd.nv + 7) / 8, K / kSlice), 256, 0, st>>>(fd, u, div, K, ground);
+    if (K % 128 == 0)
+        k_div_mixed<2><<<dim3((fd.nv + 7) / 8, K / 128), 256, 0, st>>>(fd, u, div, K, ground);
+    else  // K is a multiple of 64
+        k_div_mixed<1><<<dim3((fd.nv + 7) / 8, K / 64), 256, 0, st>>>(fd, u, div, K, ground);
 }
 
 }  // namespace fcw

@@ -99,6 +99,12 @@ struct FaceData {
     const int32_t* inc_ptr = nullptr;   // nv+1, per elimination-order vertex
     const int32_t* inc_face = nullptr;  // incident faces in ascending face order
     const int8_t* inc_corner = nullptr; // which corner of the face the vertex is
+    // the same incidences as records for the mixed form: the face's corners, its
+    // FP32 intrinsic coefficients (c11, c12, c22, area) and the vertex's corner
+    // weights (w1, w2), so a vertex reads its faces without an index chain
+    const int4* inc_corners = nullptr;
+    const float4* inc_coef = nullptr;
+    const float2* inc_w = nullptr;
 };
 void launch_divergence_fp64(const FaceData& fd, const double* u, double* div, int32_t K, cudaStream_t st);
 void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,
