@@ -50,16 +50,16 @@ enum { P_SUM_D, P_SUM_DA, P_SUM_A, P_CNT, P_NEG, P_VIOL, P_NONFINITE, P_DMAX, P_
 // 1e-10 band of the threshold, so the counts match the reference exactly. Vertices
 // closer than the near radius are appended to their source's near list.
 template <typename Tin, typename Tout>
-__global__ void __launch_bounds__(256) k_shift_stats(MetricArgs a, int32_t K, const Tin* __restrict__ phi,
+__global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K, const Tin* __restrict__ phi,
                                                      Tout* __restrict__ dT) {
     __shared__ Tin tile[32][33];
     __shared__ Tin sh[32];
     __shared__ double sc[32][3];
-    __shared__ double vc[32][4];
     __shared__ int srcv[32];
     const int n = a.n;
     const int k0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const int vbase = blockIdx.x * kStatVTile;
     if (ty == 0) {
         const int sidx = a.src[k0 + tx];
         srcv[tx] = sidx;
@@ -72,22 +72,36 @@ __global__ void __launch_bounds__(256) k_shift_stats(MetricArgs a, int32_t K, co
     for (int j = 0; j < 4; ++j) { sd[j] = sda[j] = sa[j] = 0.0; dm[j] = 0.0; cnt[j] = ng[j] = vi[j] = nf[j] = 0; }
     const double h = a.health_h, R0 = a.near_radius;
     const unsigned lanes_below = (1u << tx) - 1u;
+    // the field values of the next 32-vertex sub-tile are loaded while this one is processed
+    Tin nxt[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int v = vbase + ty + 8 * j;
+        nxt[j] = v < n ? phi[(int64_t)v * K + k0 + tx] : Tin(0);
+    }
     for (int sub = 0; sub < kStatVTile / 32; ++sub) {
-        const int v0 = blockIdx.x * kStatVTile + sub * 32;
+        const int v0 = vbase + sub * 32;
         if (v0 >= n) break;
-        __syncthreads();
-        for (int r = ty; r < 32; r += 8) {
-            const int v = v0 + r;
-            tile[r][tx] = v < n ? phi[(int64_t)v * K + k0 + tx] : Tin(0);
+        __syncthreads();  // the previous sub-tile's reads of `tile` are done
+#pragma unroll
+        for (int j = 0; j < 4; ++j) tile[ty + 8 * j][tx] = nxt[j];
+        if (sub + 1 < kStatVTile / 32) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int v = v0 + 32 + ty + 8 * j;
+                nxt[j] = v < n ? phi[(int64_t)v * K + k0 + tx] : Tin(0);
+            }
         }
-        if (ty == 0 && v0 + tx < n) {
-            const int v = v0 + tx;
-            for (int c = 0; c < 3; ++c) vc[tx][c] = a.coords[3 * (int64_t)v + c];
-            vc[tx][3] = a.vertex_area[v];
-        }
-        __syncthreads();
         const int v = v0 + tx;
         const bool in = v < n;
+        double vx = 0.0, vy = 0.0, vz = 0.0, va = 0.0;
+        if (in) {
+            vx = a.coords[3 * (int64_t)v];
+            vy = a.coords[3 * (int64_t)v + 1];
+            vz = a.coords[3 * (int64_t)v + 2];
+            va = a.vertex_area[v];
+        }
+        __syncthreads();
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int r = ty + 8 * j, k = k0 + r;
@@ -101,7 +115,7 @@ __global__ void __launch_bounds__(256) k_shift_stats(MetricArgs a, int32_t K, co
                     ++nf[j];
                 } else {
                     if (di < -h) ++ng[j];
-                    const double dx = vc[tx][0] - sc[r][0], dy = vc[tx][1] - sc[r][1], dz = vc[tx][2] - sc[r][2];
+                    const double dx = vx - sc[r][0], dy = vy - sc[r][1], dz = vz - sc[r][2];
                     const double c2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
                     const double t = di + h;
                     bool viol;
@@ -115,10 +129,9 @@ __global__ void __launch_bounds__(256) k_shift_stats(MetricArgs a, int32_t K, co
                     }
                     if (viol) ++vi[j];
                     if (di > a.eps) {
-                        const double wa = vc[tx][3];
                         sd[j] += di;
-                        sda[j] += di * wa;
-                        sa[j] += wa;
+                        sda[j] += di * va;
+                        sa[j] += va;
                         ++cnt[j];
                     }
                     dm[j] = fmax(dm[j], di);
