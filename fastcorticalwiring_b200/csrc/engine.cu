@@ -109,6 +109,7 @@ struct fcw_engine {
     std::vector<int32_t> level_tiles;
     // solve schedule: per level, task ranges of the forward / backward task lists
     std::vector<int32_t> fwd_ptr, bwd_ptr;
+    std::vector<int32_t> level_rows;  // backward tile rows per level: 32 if all its supernodes are <= 32 wide
     int2 *fwd_tasks = nullptr, *bwd_tasks = nullptr;
     int64_t* uoff_d = nullptr;
     int64_t* poff_d = nullptr;
@@ -370,7 +371,16 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
         std::vector<int2> ft, bt;
         e->fwd_ptr.assign(S.nlevels + 1, 0);
         e->bwd_ptr.assign(S.nlevels + 1, 0);
+        e->level_rows.assign(S.nlevels, fcw::kMaxWidth);
         for (int32_t l = 0; l < S.nlevels; ++l) {
+            int32_t widest = 0;
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+                const int32_t s = S.level_nodes[q];
+                widest = std::max(widest, S.sn_c0[s + 1] - S.sn_c0[s]);
+            }
+            // narrow backward tiles on the leaf levels; the forward sweep keeps 64-row
+            // tasks everywhere (32-row tasks would recompute X_s for twice as many chunks)
+            e->level_rows[l] = widest <= 32 ? 32 : fcw::kMaxWidth;
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
                 const int32_t s = S.level_nodes[q];
                 const int32_t ns = S.sn_c0[s + 1] - S.sn_c0[s], nr = S.sn_m[s] - ns;
@@ -634,7 +644,7 @@ void sweep(fcw_engine* e, fcw::SolveArgs<T> a, cudaStream_t st, int stage_fwd, i
     mark(e, st, stage_bwd);
     for (int32_t l = S.nlevels - 1; l >= 0; --l) {
         a.tasks = e->bwd_tasks;
-        fcw::launch_bwd_level<T>(a, e->bwd_ptr[l], e->bwd_ptr[l + 1] - e->bwd_ptr[l], st);
+        fcw::launch_bwd_level<T>(a, e->bwd_ptr[l], e->bwd_ptr[l + 1] - e->bwd_ptr[l], e->level_rows[l], st);
     }
     e->launches += 2 * (int64_t)S.nlevels;
 }

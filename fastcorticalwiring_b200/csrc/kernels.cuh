@@ -84,9 +84,10 @@ cudaError_t configure_solve_kernels();
 // Forward sweep of one level (tasks [t0, t0+ntasks) of the level's list).
 template <typename T>
 void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st);
-// Backward sweep of one level.
+// Backward sweep of one level; tile_rows is 32 when every supernode of the
+// level is at most 32 wide, else 64.
 template <typename T>
-void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st);
+void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, int32_t tile_rows, cudaStream_t st);
 void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st);
 
 // ---- fused gradient -> normalise -> divergence (face.cu) ----

@@ -272,17 +272,24 @@ struct Field {
         double x1 = 0.0, x2 = 0.0;
         const int* fv = a->fv;
         if (kend <= s->rc) {
-            // two records per lane in flight
+            // four records per lane in flight
             int j = s->ptr[kr] + lane;
             const int je = s->ptr[kend];
-            for (; j + 32 < je; j += 64) {
-                const int4 q0 = band[j], q1 = band[j + 32];
-                const double a0 = dv(q0.y), a1 = dv(q0.z), a2 = dv(q0.w);
-                const double b0 = dv(q1.y), b1 = dv(q1.z), b2 = dv(q1.w);
-                rec_term(q0, a0, a1, a2, r, mode, x1, x2);
-                rec_term(q1, b0, b1, b2, r, mode, x1, x2);
+            for (; j + 96 < je; j += 128) {
+                int4 q[4];
+                double dd[4][3];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) q[u] = band[j + 32 * u];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    dd[u][0] = dv(q[u].y);
+                    dd[u][1] = dv(q[u].z);
+                    dd[u][2] = dv(q[u].w);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) rec_term(q[u], dd[u][0], dd[u][1], dd[u][2], r, mode, x1, x2);
             }
-            if (j < je) {
+            for (; j < je; j += 32) {
                 const int4 q0 = band[j];
                 rec_term(q0, dv(q0.y), dv(q0.z), dv(q0.w), r, mode, x1, x2);
             }

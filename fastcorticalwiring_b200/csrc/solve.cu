@@ -37,6 +37,8 @@
 // Heat right-hand sides are columns of the identity: the forward sweep builds
 // them from the source list, and only supernodes on a source's path to the
 // root (`reach`) are solved; the others' forward results are zero.
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace fcw {
@@ -44,26 +46,30 @@ namespace fcw {
 namespace {
 
 constexpr int NT = 256;         // threads per CTA
-constexpr int TR = kMaxWidth;   // rows of a tile (= widest supernode)
+constexpr int PT = kMaxWidth;   // rows of a backward partial-sum slot (= widest supernode)
 constexpr int RC = 32;          // structure rows per backward chunk
+// Tiles are TR = 64 rows (any supernode); the backward sweep also has TR = 32
+// for the levels whose supernodes are all at most 32 wide (the leaves), where
+// smaller tiles and accumulators let three CTAs share an SM.
 
 // Column tile of each precision when K allows it (512-byte rows).
 template <typename T>
 constexpr int wide_tile() { return sizeof(T) == 4 ? 128 : 64; }
-// Children's update rows staged per forward gather chunk (two CTAs per SM).
-template <typename T>
-constexpr int stage_rows() { return sizeof(T) == 4 ? 112 : 80; }
+// Children's update rows staged per forward gather chunk (two CTAs per SM with
+// 64-row tiles, three with 32-row tiles).
+template <typename T, int TR>
+constexpr int stage_rows() { return TR == 32 ? 96 : (sizeof(T) == 4 ? 112 : 80); }
 template <typename T>
 constexpr int vec() { return 16 / (int)sizeof(T); }  // elements per 16-byte vector
 
 // Shared-tile leading dimensions, chosen so that the product's operand reads
 // are free of bank conflicts: FP64 tensor fragments read 8 rows x 4 depths
-// (row stride 68 doubles = 8 banks apart), FP32 register tiles read rows ty and
+// (row stride TR + 4 doubles = 8 banks apart), FP32 register tiles read rows ty and
 // ty+1 of a row-major A (odd stride) or adjacent columns of a transposed one.
-template <typename T>
-constexpr int ld_fwd_a() { return sizeof(T) == 8 ? 68 : TR + 1; }  // forward inverse / panel, row-major
-template <typename T>
-constexpr int ld_bwd_a() { return sizeof(T) == 8 ? 68 : TR; }      // backward panel / inverse, transposed
+template <typename T, int TR>
+constexpr int ld_fwd_a() { return sizeof(T) == 8 ? TR + 4 : TR + 1; }  // forward inverse / panel, row-major
+template <typename T, int TR>
+constexpr int ld_bwd_a() { return sizeof(T) == 8 ? TR + 4 : TR; }      // backward panel / inverse, transposed
 template <typename T, int KT>
 constexpr int ld_rows() { return sizeof(T) == 8 ? KT + 4 : KT; }    // right-hand-side rows (W, X, C, gathers)
 template <typename T>
@@ -117,21 +123,34 @@ __device__ __forceinline__ void st_n(T* p, const T* w) {
 // f(row, col, T* v), v holding V adjacent columns.
 // ---------------------------------------------------------------------------
 
-// FP32 register tiles: thread (ty, tx) owns rows ty + 16a and 16-byte column
-// groups at vec*tx + 16*vec*h.
-template <typename T, int KT>
+// Calls f(std::integral_constant<int, m>) with m = min(n, N), for n >= 1: the row
+// blocks a product needs, as a compile-time count.
+template <int N, class F>
+__device__ __forceinline__ void upto(int n, F&& f) {
+    if constexpr (N > 1) {
+        if (n < N) {
+            upto<N - 1>(n, f);
+            return;
+        }
+    }
+    f(std::integral_constant<int, N>{});
+}
+
+// FP32 register tiles: thread (ty, tx) owns rows ty + 16a (a < NA) and 16-byte
+// column groups at vec*tx + 16*vec*h.
+template <typename T, int KT, int NA>
 struct AccScalar {
     static constexpr int NB = KT / 16, G = vec<T>(), V = G;
-    T c[4][NB];
+    T c[NA][NB];
 
     __device__ __forceinline__ void zero() {
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int b = 0; b < NB; ++b) c[a][b] = T(0);
     }
 
-    template <int NA>
+    template <int MA>
     __device__ __forceinline__ void rows_n(const T* A, int lda, const T* Bm, int ldb, int depth) {
         const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
         const T* ap = A + ty * lda;
@@ -141,7 +160,7 @@ struct AccScalar {
 #pragma unroll
             for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
 #pragma unroll
-            for (int a = 0; a < NA; ++a) {
+            for (int a = 0; a < MA; ++a) {
                 const T l = ap[16 * a * lda + j];
 #pragma unroll
                 for (int b = 0; b < NB; ++b) c[a][b] += l * w[b];
@@ -149,18 +168,18 @@ struct AccScalar {
         }
     }
 
-    template <int NA>
+    template <int MA>
     __device__ __forceinline__ void cols_n(const T* A, int lda, const T* Bm, int ldb, int depth) {
         const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
         const T* bp = Bm + G * tx;
         for (int j = 0; j < depth; ++j) {
-            T w[NB], l[NA];
+            T w[NB], l[MA];
 #pragma unroll
             for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
 #pragma unroll
-            for (int a = 0; a < NA; ++a) l[a] = A[j * lda + ty + 16 * a];
+            for (int a = 0; a < MA; ++a) l[a] = A[j * lda + ty + 16 * a];
 #pragma unroll
-            for (int a = 0; a < NA; ++a)
+            for (int a = 0; a < MA; ++a)
 #pragma unroll
                 for (int b = 0; b < NB; ++b) c[a][b] += l[a] * w[b];
         }
@@ -168,29 +187,19 @@ struct AccScalar {
 
     // only the 16-row blocks holding one of the first nrows rows are computed
     __device__ __forceinline__ void rows(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
-        switch ((nrows + 15) >> 4) {
-            case 0: break;
-            case 1: rows_n<1>(A, lda, Bm, ldb, depth); break;
-            case 2: rows_n<2>(A, lda, Bm, ldb, depth); break;
-            case 3: rows_n<3>(A, lda, Bm, ldb, depth); break;
-            default: rows_n<4>(A, lda, Bm, ldb, depth); break;
-        }
+        const int na = (nrows + 15) >> 4;
+        if (na > 0) upto<NA>(na, [&](auto m) { rows_n<decltype(m)::value>(A, lda, Bm, ldb, depth); });
     }
     __device__ __forceinline__ void cols(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
-        switch ((nrows + 15) >> 4) {
-            case 0: break;
-            case 1: cols_n<1>(A, lda, Bm, ldb, depth); break;
-            case 2: cols_n<2>(A, lda, Bm, ldb, depth); break;
-            case 3: cols_n<3>(A, lda, Bm, ldb, depth); break;
-            default: cols_n<4>(A, lda, Bm, ldb, depth); break;
-        }
+        const int na = (nrows + 15) >> 4;
+        if (na > 0) upto<NA>(na, [&](auto m) { cols_n<decltype(m)::value>(A, lda, Bm, ldb, depth); });
     }
 
     template <class F>
     __device__ __forceinline__ void visit(int nrows, F&& f) {
         const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
+        for (int a = 0; a < NA; ++a) {
             const int t = ty + 16 * a;
             if (t < nrows)
 #pragma unroll
@@ -200,16 +209,17 @@ struct AccScalar {
 };
 
 // FP64 tensor tiles (KT = 64): warp w owns columns [8w, 8w+8) and the 8-row
-// m8n8k4 tiles down to row 64; lane (g = lane/4, t = lane%4) holds rows 8m+g,
+// m8n8k4 tiles down to row 8*MT; lane (g = lane/4, t = lane%4) holds rows 8m+g,
 // columns 8w+2t and 8w+2t+1. The depth must be a multiple of 4 with the padded
 // depths zero in both operands.
+template <int MT>
 struct AccDmma {
     static constexpr int V = 2;
-    double c[8][2];
+    double c[MT][2];
 
     __device__ __forceinline__ void zero() {
 #pragma unroll
-        for (int m = 0; m < 8; ++m) c[m][0] = c[m][1] = 0.0;
+        for (int m = 0; m < MT; ++m) c[m][0] = c[m][1] = 0.0;
     }
 
     static __device__ __forceinline__ void mma(double (&d)[2], double a, double b) {
@@ -218,14 +228,14 @@ struct AccDmma {
             : "d"(a), "d"(b));
     }
 
-    template <int MT, bool TRANS>
+    template <int MM, bool TRANS>
     __device__ __forceinline__ void run(const double* A, int lda, const double* Bm, int ldb, int depth) {
         const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, n0 = 8 * (threadIdx.x >> 5);
         const double* bp = Bm + t * ldb + n0 + g;
         for (int k = 0; k < depth; k += 4) {
             const double b = bp[k * ldb];
 #pragma unroll
-            for (int m = 0; m < MT; ++m) {
+            for (int m = 0; m < MM; ++m) {
                 const double a = TRANS ? A[(k + t) * lda + 8 * m + g] : A[(8 * m + g) * lda + k + t];
                 mma(c[m], a, b);
             }
@@ -235,17 +245,8 @@ struct AccDmma {
     template <bool TRANS>
     __device__ __forceinline__ void dispatch(const double* A, int lda, const double* Bm, int ldb, int depth,
                                              int nrows) {
-        switch ((nrows + 7) >> 3) {
-            case 0: break;
-            case 1: run<1, TRANS>(A, lda, Bm, ldb, depth); break;
-            case 2: run<2, TRANS>(A, lda, Bm, ldb, depth); break;
-            case 3: run<3, TRANS>(A, lda, Bm, ldb, depth); break;
-            case 4: run<4, TRANS>(A, lda, Bm, ldb, depth); break;
-            case 5: run<5, TRANS>(A, lda, Bm, ldb, depth); break;
-            case 6: run<6, TRANS>(A, lda, Bm, ldb, depth); break;
-            case 7: run<7, TRANS>(A, lda, Bm, ldb, depth); break;
-            default: run<8, TRANS>(A, lda, Bm, ldb, depth); break;
-        }
+        const int nm = (nrows + 7) >> 3;
+        if (nm > 0) upto<MT>(nm, [&](auto m) { run<decltype(m)::value, TRANS>(A, lda, Bm, ldb, depth); });
     }
     __device__ __forceinline__ void rows(const double* A, int lda, const double* Bm, int ldb, int depth,
                                          int nrows) {
@@ -260,21 +261,21 @@ struct AccDmma {
     __device__ __forceinline__ void visit(int nrows, F&& f) {
         const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, n0 = 8 * (threadIdx.x >> 5);
 #pragma unroll
-        for (int m = 0; m < 8; ++m)
+        for (int m = 0; m < MT; ++m)
             if (8 * m + g < nrows) f(8 * m + g, n0 + 2 * t, c[m]);
     }
 };
 
-template <typename T, int KT>
+template <typename T, int KT, int TR>
 struct AccSel {
-    using type = AccScalar<T, KT>;
+    using type = AccScalar<T, KT, TR / 16>;
 };
-template <>
-struct AccSel<double, 64> {
-    using type = AccDmma;
+template <int TR>
+struct AccSel<double, 64, TR> {
+    using type = AccDmma<TR / 8>;
 };
-template <typename T, int KT>
-using Acc = typename AccSel<T, KT>::type;
+template <typename T, int KT, int TR>
+using Acc = typename AccSel<T, KT, TR>::type;
 
 // Zero rows [r0, r1) x columns [0, ncols) of a shared tile (padding of a product's depth).
 template <typename T>
@@ -343,10 +344,10 @@ __device__ __forceinline__ GatherRange gather_open(const SolveArgs<T>& a, int64_
 
 // Async copies of the staged chunk that starts at entry e0; live[e] = 0 for rows
 // of children off the sources' paths (their update rows were never written).
-template <typename T, int KT>
+template <typename T, int KT, int TR>
 __device__ __forceinline__ void gather_issue(const SolveArgs<T>& a, const GatherRange& g, int e0, int k0, T* St,
                                              unsigned char* live) {
-    constexpr int VPR = KT / vec<T>(), SG = stage_rows<T>();
+    constexpr int VPR = KT / vec<T>(), SG = stage_rows<T, TR>();
     const int ne = min(g.E - e0, SG);
     for (int i = threadIdx.x; i < ne * VPR; i += NT) {
         const int e = i / VPR, v = i - e * VPR;
@@ -380,14 +381,14 @@ __device__ __forceinline__ void gather_accumulate(T* D, int ld, const T* St, con
 
 // Waits for every copy this CTA has in flight (the caller has issued the
 // range's first chunk), then adds the range chunk by chunk.
-template <typename T, int KT, bool SUB>
+template <typename T, int KT, int TR, bool SUB>
 __device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const GatherRange& g, int k0, T* D, int ld,
                                               int nrows, T* St, unsigned char* live, const int* grs) {
-    constexpr int SG = stage_rows<T>();
+    constexpr int SG = stage_rows<T, TR>();
     int e0 = 0;
     do {
         if (e0 > 0) {
-            gather_issue<T, KT>(a, g, e0, k0, St, live);
+            gather_issue<T, KT, TR>(a, g, e0, k0, St, live);
             copy_async_commit();
         }
         copy_async_wait();
@@ -398,15 +399,16 @@ __device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const Gathe
     } while (e0 < g.E);
 }
 
-template <typename T, int KT>
-__global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
-    constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_fwd_a<T>(), DP = depth_pad<T>();
+template <typename T, int KT, int TR>
+__global__ void __launch_bounds__(NT, TR == 32 ? 3 : 2) k_fwd(SolveArgs<T> a, int32_t t0) {
+    constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_fwd_a<T, TR>(), DP = depth_pad<T>();
+    using AccT = Acc<T, KT, TR>;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* Wt = reinterpret_cast<T*>(smraw);   // TR x LW: W, then X, then this chunk's update rows
     T* Lp = Wt + TR * LW;                   // TR x LA: inverse diagonal block, then the panel chunk
     T* St = Lp + TR * LA;                   // stage_rows x KT: children's update rows
     __shared__ int grs[TR + 1];
-    __shared__ unsigned char live[stage_rows<T>()];
+    __shared__ unsigned char live[stage_rows<T, TR>()];
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, chunk = task.y;
     if (a.reach && !a.reach[s]) return;
@@ -442,16 +444,16 @@ __global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
         zero_cols(Lp, LA, ns, ns, nsp);
     }
     const GatherRange g1 = gather_open(a, fb, 0, ns, grs);
-    if (g1.E > 0) gather_issue<T, KT>(a, g1, 0, k0, St, live);
+    if (g1.E > 0) gather_issue<T, KT, TR>(a, g1, 0, k0, St, live);
     copy_async_commit();
-    gather_finish<T, KT, true>(a, g1, k0, Wt, LW, ns, St, live, grs);
+    gather_finish<T, KT, TR, true>(a, g1, k0, Wt, LW, ns, St, live, grs);
 
     // X = inv(L_ss) W, written over W
-    Acc<T, KT> acc;
+    AccT acc;
     acc.zero();
     acc.rows(Lp, LA, Wt, LW, nsp, ns);
     __syncthreads();
-    acc.visit(ns, [&](int r, int c, T* v) { st_n<T, Acc<T, KT>::V>(Wt + r * LW + c, v); });
+    acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(Wt + r * LW + c, v); });
     __syncthreads();
     if (chunk == 0) tile_rows_to_global<T, KT>(a.B + (int64_t)c0 * K + k0, K, Wt, LW, ns);
     if (nq <= 0) return;
@@ -465,24 +467,24 @@ __global__ void __launch_bounds__(NT, 2) k_fwd(SolveArgs<T> a, int32_t t0) {
     }
     if (nsp > ns) zero_cols(Lp, LA, nq, ns, nsp);
     const GatherRange g2 = gather_open(a, fb, ns + q0, nq, grs);
-    if (g2.E > 0) gather_issue<T, KT>(a, g2, 0, k0, St, live);
+    if (g2.E > 0) gather_issue<T, KT, TR>(a, g2, 0, k0, St, live);
     copy_async_commit();
     copy_async_wait();
     __syncthreads();
     acc.zero();
     acc.rows(Lp, LA, Wt, LW, nsp, nq);
     __syncthreads();
-    acc.visit(nq, [&](int r, int c, T* v) { st_n<T, Acc<T, KT>::V>(Wt + r * LW + c, v); });
-    gather_finish<T, KT, false>(a, g2, k0, Wt, LW, nq, St, live, grs);
+    acc.visit(nq, [&](int r, int c, T* v) { st_n<T, AccT::V>(Wt + r * LW + c, v); });
+    gather_finish<T, KT, TR, false>(a, g2, k0, Wt, LW, nq, St, live, grs);
     tile_rows_to_global<T, KT>(a.U + (a.uoff[s] + q0) * (int64_t)K + k0, K, Wt, LW, nq);
 }
 
-template <typename T, int KT>
-__global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
-    constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_bwd_a<T>(), DP = depth_pad<T>();
+template <typename T, int KT, int TR>
+__global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
+    constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_bwd_a<T, TR>(), DP = depth_pad<T>();
     constexpr int PS = RC * LA, XS = RC * LW;  // one chunk buffer: panel rows, gathered solution rows
     static_assert(2 * (PS + XS) >= TR * LW + TR * LA, "the finishing tiles alias the chunk buffers");
-    using AccT = Acc<T, KT>;
+    using AccT = Acc<T, KT, TR>;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* buf = reinterpret_cast<T*>(smraw);
     T* Cs = buf;             // TR x LW, after the gather
@@ -539,8 +541,8 @@ __global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
 
     const bool zero_y = a.reach && !a.reach[s];
     if (nspl > 1) {
-        T* part = a.part + a.poff[s] * (int64_t)TR * K + k0;
-        T* mine = part + (int64_t)split * TR * K;
+        T* part = a.part + a.poff[s] * (int64_t)PT * K + k0;
+        T* mine = part + (int64_t)split * PT * K;
         acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(mine + (int64_t)r * K + c, v); });
         __threadfence();
         __syncthreads();
@@ -555,7 +557,7 @@ __global__ void __launch_bounds__(NT) k_bwd(SolveArgs<T> a, int32_t t0) {
 #pragma unroll
             for (int q = 0; q < AccT::V; ++q) {
                 T sum = T(0);
-                for (int sp = 0; sp < nspl; ++sp) sum += __ldcg(&part[((int64_t)sp * TR + r) * K + c + q]);
+                for (int sp = 0; sp < nspl; ++sp) sum += __ldcg(&part[((int64_t)sp * PT + r) * K + c + q]);
                 v[q] = sum;
             }
         });
@@ -603,21 +605,35 @@ __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __res
     }
 }
 
-template <typename T, int KT>
+template <typename T, int KT, int TR>
 constexpr size_t fwd_smem() {
-    return (size_t)(TR * ld_rows<T, KT>() + TR * ld_fwd_a<T>() + stage_rows<T>() * KT) * sizeof(T);
+    return (size_t)(TR * ld_rows<T, KT>() + TR * ld_fwd_a<T, TR>() + stage_rows<T, TR>() * KT) * sizeof(T);
 }
-template <typename T, int KT>
+template <typename T, int KT, int TR>
 constexpr size_t bwd_smem() {
-    return (size_t)2 * (RC * ld_bwd_a<T>() + RC * ld_rows<T, KT>()) * sizeof(T);
+    return (size_t)2 * (RC * ld_bwd_a<T, TR>() + RC * ld_rows<T, KT>()) * sizeof(T);
 }
 
+// forward sweeps run 64-row tiles; backward sweeps 64- or 32-row tiles
 template <typename T, int KT>
 cudaError_t set_smem() {
-    cudaError_t e = cudaFuncSetAttribute(k_fwd<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)fwd_smem<T, KT>());
+    cudaError_t e = cudaFuncSetAttribute(k_fwd<T, KT, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fwd_smem<T, KT, 64>());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_bwd<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem<T, KT>());
+    e = cudaFuncSetAttribute(k_bwd<T, KT, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bwd_smem<T, KT, 64>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_bwd<T, KT, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bwd_smem<T, KT, 32>());
+}
+
+template <typename T, int KT, int TR>
+void fwd_launch(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
+    k_fwd<T, KT, TR><<<dim3(ntasks, a.K / KT), NT, fwd_smem<T, KT, TR>(), st>>>(a, t0);
+}
+template <typename T, int KT, int TR>
+void bwd_launch(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
+    k_bwd<T, KT, TR><<<dim3(ntasks, a.K / KT), NT, bwd_smem<T, KT, TR>(), st>>>(a, t0);
 }
 
 }  // namespace
@@ -634,19 +650,20 @@ void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStr
     if (ntasks <= 0 || a.K <= 0) return;
     constexpr int W = wide_tile<T>();
     if (W != 64 && a.K % W == 0)
-        k_fwd<T, W><<<dim3(ntasks, a.K / W), NT, fwd_smem<T, W>(), st>>>(a, t0);
+        fwd_launch<T, W, 64>(a, t0, ntasks, st);
     else
-        k_fwd<T, 64><<<dim3(ntasks, a.K / 64), NT, fwd_smem<T, 64>(), st>>>(a, t0);
+        fwd_launch<T, 64, 64>(a, t0, ntasks, st);
 }
 
 template <typename T>
-void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
+void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, int32_t tile_rows, cudaStream_t st) {
     if (ntasks <= 0 || a.K <= 0) return;
     constexpr int W = wide_tile<T>();
-    if (W != 64 && a.K % W == 0)
-        k_bwd<T, W><<<dim3(ntasks, a.K / W), NT, bwd_smem<T, W>(), st>>>(a, t0);
+    const bool wide = W != 64 && a.K % W == 0;
+    if (tile_rows == 32)
+        wide ? bwd_launch<T, W, 32>(a, t0, ntasks, st) : bwd_launch<T, 64, 32>(a, t0, ntasks, st);
     else
-        k_bwd<T, 64><<<dim3(ntasks, a.K / 64), NT, bwd_smem<T, 64>(), st>>>(a, t0);
+        wide ? bwd_launch<T, W, 64>(a, t0, ntasks, st) : bwd_launch<T, 64, 64>(a, t0, ntasks, st);
 }
 
 void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st) {
@@ -656,7 +673,7 @@ void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reac
 
 template void launch_fwd_level<double>(const SolveArgs<double>&, int32_t, int32_t, cudaStream_t);
 template void launch_fwd_level<float>(const SolveArgs<float>&, int32_t, int32_t, cudaStream_t);
-template void launch_bwd_level<double>(const SolveArgs<double>&, int32_t, int32_t, cudaStream_t);
-template void launch_bwd_level<float>(const SolveArgs<float>&, int32_t, int32_t, cudaStream_t);
+template void launch_bwd_level<double>(const SolveArgs<double>&, int32_t, int32_t, int32_t, cudaStream_t);
+template void launch_bwd_level<float>(const SolveArgs<float>&, int32_t, int32_t, int32_t, cudaStream_t);
 
 }  // namespace fcw
