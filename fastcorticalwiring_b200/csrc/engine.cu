@@ -110,6 +110,7 @@ struct fcw_engine {
     // solve schedule: per level, task ranges of the forward / backward task lists
     std::vector<int32_t> fwd_ptr, bwd_ptr;
     std::vector<int32_t> level_rows;  // backward tile rows per level: 32 if all its supernodes are <= 32 wide
+    std::vector<uint8_t> level_gathers;  // some supernode of the level has children
     int2 *fwd_tasks = nullptr, *bwd_tasks = nullptr;
     int64_t* uoff_d = nullptr;
     int64_t* poff_d = nullptr;
@@ -372,11 +373,13 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
         e->fwd_ptr.assign(S.nlevels + 1, 0);
         e->bwd_ptr.assign(S.nlevels + 1, 0);
         e->level_rows.assign(S.nlevels, fcw::kMaxWidth);
+        e->level_gathers.assign(S.nlevels, 0);
         for (int32_t l = 0; l < S.nlevels; ++l) {
             int32_t widest = 0;
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
                 const int32_t s = S.level_nodes[q];
                 widest = std::max(widest, S.sn_c0[s + 1] - S.sn_c0[s]);
+                if (S.child_ptr[s + 1] > S.child_ptr[s]) e->level_gathers[l] = 1;
             }
             // narrow backward tiles on the leaf levels; the forward sweep keeps 64-row
             // tasks everywhere (32-row tasks would recompute X_s for twice as many chunks)
@@ -638,7 +641,7 @@ void sweep(fcw_engine* e, fcw::SolveArgs<T> a, cudaStream_t st, int stage_fwd, i
     mark(e, st, stage_fwd);
     for (int32_t l = 0; l < S.nlevels; ++l) {
         a.tasks = e->fwd_tasks;
-        fcw::launch_fwd_level<T>(a, e->fwd_ptr[l], e->fwd_ptr[l + 1] - e->fwd_ptr[l], st);
+        fcw::launch_fwd_level<T>(a, e->fwd_ptr[l], e->fwd_ptr[l + 1] - e->fwd_ptr[l], e->level_gathers[l] != 0, st);
     }
     a.delta_src = nullptr;
     mark(e, st, stage_bwd);

@@ -78,12 +78,15 @@ struct SolveArgs {
     T* part = nullptr;
     int* counters = nullptr;             // per (supernode, column tile) arrival tickets, zero at rest
     int32_t ktiles = 0;                  // column tiles the counters were sized for
+    int32_t stage = 0;                   // forward: children's update rows staged per chunk (set by the launcher)
 };
 
 cudaError_t configure_solve_kernels();
-// Forward sweep of one level (tasks [t0, t0+ntasks) of the level's list).
+// Forward sweep of one level (tasks [t0, t0+ntasks) of the level's list);
+// gathers: some supernode of the level has children (leaf levels have none and
+// launch without a staging buffer, so more CTAs share an SM).
 template <typename T>
-void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st);
+void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, bool gathers, cudaStream_t st);
 // Backward sweep of one level; tile_rows is 32 when every supernode of the
 // level is at most 32 wide, else 64.
 template <typename T>

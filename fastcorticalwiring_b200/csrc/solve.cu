@@ -55,10 +55,13 @@ constexpr int RC = 32;          // structure rows per backward chunk
 // Column tile of each precision when K allows it (512-byte rows).
 template <typename T>
 constexpr int wide_tile() { return sizeof(T) == 4 ? 128 : 64; }
-// Children's update rows staged per forward gather chunk (two CTAs per SM with
-// 64-row tiles, three with 32-row tiles).
+// Most children's update rows a forward CTA stages per gather chunk. The
+// launcher picks the count per level (SolveArgs::stage): none on levels without
+// children, else what keeps three FP32 CTAs (two FP64) on an SM.
 template <typename T, int TR>
-constexpr int stage_rows() { return TR == 32 ? 96 : (sizeof(T) == 4 ? 112 : 80); }
+constexpr int stage_rows() { return sizeof(T) == 4 ? 112 : 80; }
+template <typename T, int KT>
+constexpr int stage_used() { return sizeof(T) == 8 ? 80 : (KT == 128 ? 48 : 112); }
 template <typename T>
 constexpr int vec() { return 16 / (int)sizeof(T); }  // elements per 16-byte vector
 
@@ -347,8 +350,8 @@ __device__ __forceinline__ GatherRange gather_open(const SolveArgs<T>& a, int64_
 template <typename T, int KT, int TR>
 __device__ __forceinline__ void gather_issue(const SolveArgs<T>& a, const GatherRange& g, int e0, int k0, T* St,
                                              unsigned char* live) {
-    constexpr int VPR = KT / vec<T>(), SG = stage_rows<T, TR>();
-    const int ne = min(g.E - e0, SG);
+    constexpr int VPR = KT / vec<T>();
+    const int ne = min(g.E - e0, a.stage);
     for (int i = threadIdx.x; i < ne * VPR; i += NT) {
         const int e = i / VPR, v = i - e * VPR;
         const int ge = g.eb + e0 + e;
@@ -384,7 +387,7 @@ __device__ __forceinline__ void gather_accumulate(T* D, int ld, const T* St, con
 template <typename T, int KT, int TR, bool SUB>
 __device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const GatherRange& g, int k0, T* D, int ld,
                                               int nrows, T* St, unsigned char* live, const int* grs) {
-    constexpr int SG = stage_rows<T, TR>();
+    const int SG = a.stage;  // >= 1 whenever the level has gathers (g.E > 0)
     int e0 = 0;
     do {
         if (e0 > 0) {
@@ -400,13 +403,13 @@ __device__ __forceinline__ void gather_finish(const SolveArgs<T>& a, const Gathe
 }
 
 template <typename T, int KT, int TR>
-__global__ void __launch_bounds__(NT, TR == 32 ? 3 : 2) k_fwd(SolveArgs<T> a, int32_t t0) {
+__global__ void __launch_bounds__(NT, 3) k_fwd(SolveArgs<T> a, int32_t t0) {
     constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_fwd_a<T, TR>(), DP = depth_pad<T>();
     using AccT = Acc<T, KT, TR>;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* Wt = reinterpret_cast<T*>(smraw);   // TR x LW: W, then X, then this chunk's update rows
     T* Lp = Wt + TR * LW;                   // TR x LA: inverse diagonal block, then the panel chunk
-    T* St = Lp + TR * LA;                   // stage_rows x KT: children's update rows
+    T* St = Lp + TR * LA;                   // a.stage x KT: children's update rows
     __shared__ int grs[TR + 1];
     __shared__ unsigned char live[stage_rows<T, TR>()];
     const int2 task = a.tasks[t0 + blockIdx.x];
@@ -606,8 +609,8 @@ __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __res
 }
 
 template <typename T, int KT, int TR>
-constexpr size_t fwd_smem() {
-    return (size_t)(TR * ld_rows<T, KT>() + TR * ld_fwd_a<T, TR>() + stage_rows<T, TR>() * KT) * sizeof(T);
+constexpr size_t fwd_smem(int stage = stage_rows<T, TR>()) {
+    return (size_t)(TR * ld_rows<T, KT>() + TR * ld_fwd_a<T, TR>() + stage * KT) * sizeof(T);
 }
 template <typename T, int KT, int TR>
 constexpr size_t bwd_smem() {
@@ -628,8 +631,10 @@ cudaError_t set_smem() {
 }
 
 template <typename T, int KT, int TR>
-void fwd_launch(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
-    k_fwd<T, KT, TR><<<dim3(ntasks, a.K / KT), NT, fwd_smem<T, KT, TR>(), st>>>(a, t0);
+void fwd_launch(const SolveArgs<T>& args, int32_t t0, int32_t ntasks, bool gathers, cudaStream_t st) {
+    SolveArgs<T> a = args;
+    a.stage = gathers ? stage_used<T, KT>() : 0;
+    k_fwd<T, KT, TR><<<dim3(ntasks, a.K / KT), NT, fwd_smem<T, KT, TR>(a.stage), st>>>(a, t0);
 }
 template <typename T, int KT, int TR>
 void bwd_launch(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
@@ -646,13 +651,13 @@ cudaError_t configure_solve_kernels() {
 }
 
 template <typename T>
-void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, cudaStream_t st) {
+void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, bool gathers, cudaStream_t st) {
     if (ntasks <= 0 || a.K <= 0) return;
     constexpr int W = wide_tile<T>();
     if (W != 64 && a.K % W == 0)
-        fwd_launch<T, W, 64>(a, t0, ntasks, st);
+        fwd_launch<T, W, 64>(a, t0, ntasks, gathers, st);
     else
-        fwd_launch<T, 64, 64>(a, t0, ntasks, st);
+        fwd_launch<T, 64, 64>(a, t0, ntasks, gathers, st);
 }
 
 template <typename T>
@@ -671,8 +676,8 @@ void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reac
     k_reach<<<(K + 127) / 128, 128, 0, st>>>(p.col_sn, p.sn_parent, src, K, p.nlevels, reach);
 }
 
-template void launch_fwd_level<double>(const SolveArgs<double>&, int32_t, int32_t, cudaStream_t);
-template void launch_fwd_level<float>(const SolveArgs<float>&, int32_t, int32_t, cudaStream_t);
+template void launch_fwd_level<double>(const SolveArgs<double>&, int32_t, int32_t, bool, cudaStream_t);
+template void launch_fwd_level<float>(const SolveArgs<float>&, int32_t, int32_t, bool, cudaStream_t);
 template void launch_bwd_level<double>(const SolveArgs<double>&, int32_t, int32_t, int32_t, cudaStream_t);
 template void launch_bwd_level<float>(const SolveArgs<float>&, int32_t, int32_t, int32_t, cudaStream_t);
 
