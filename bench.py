@@ -474,7 +474,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=4096, help="sources per step")
     ap.add_argument("--block-k", type=int, default=1024)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
-    ap.add_argument("--pipeline-depth", type=int, default=2, help="blocks in flight on separate streams")
+    ap.add_argument("--pipeline-depth", type=int, default=3, help="blocks in flight on separate streams")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--cpu-sample", type=int, default=24, help="sources timed on the CPU oracle (0 = skip)")
     ap.add_argument("--cpu-timeout", type=float, default=600.0)

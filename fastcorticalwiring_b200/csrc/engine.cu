@@ -803,7 +803,7 @@ void fcw_default_params(fcw_params* p) {
     p->relax = 32;
     p->build_mixed = 1;
     p->device = 0;
-    p->pipeline_depth = 2;
+    p->pipeline_depth = 3;
 }
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between) {
