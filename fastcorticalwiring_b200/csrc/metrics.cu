@@ -390,7 +390,7 @@ struct Field {
 //      rc grows (up to every bin, scanning all vertices) and step 2 repeats;
 //   3. one warp per target: bracket + safeguarded Newton + perimeter; then the samples.
 template <typename T>
-__global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
+__global__ void __launch_bounds__(512, 2) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
     __shared__ SrcShared S;
     const int k = blockIdx.x;
     const int src = a.src[k];
@@ -496,28 +496,53 @@ __global__ void __launch_bounds__(512) k_source_metrics(MetricArgs a, const T* _
                 const int i = listed ? nl[ii] : ii;
                 const double di = (double)d[i];
                 if (!(di < R)) continue;
-                for (int q = a.inc_ptr[i]; q < a.inc_ptr[i + 1]; ++q) {
-                    const int4 rec = a.inc_rec[q];
-                    const int f = rec.x;
-                    const int c = a.inc_corner[q];
-                    const double d0 = (double)d[rec.y], d1 = (double)d[rec.z], d2 = (double)d[rec.w];
-                    if (c >= 1 && d0 < R) continue;   // an earlier corner emits it
-                    if (c == 2 && d1 < R) continue;
-                    if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
-                    double lo = d0, hi = d0;
-                    if (d1 < lo) lo = d1;
-                    if (d1 > hi) hi = d1;
-                    if (d2 < lo) lo = d2;
-                    if (d2 > hi) hi = d2;
-                    const int kb = F.bin_of(hi);
-                    if (pass == 0) {
-                        if (hi - lo > w) longf[atomicAdd(&S.nlong, 1)] = f;
-                        if (kb <= rc && kb < kMaxBins) {
-                            atomicAdd(&S.hist[kb], (unsigned long long)a.farea_fx[f]);
-                            atomicAdd(&S.ptr[kb], 1);
+                const int q1 = a.inc_ptr[i + 1];
+                constexpr int QB = sizeof(T) == 4 ? 4 : 2;
+                // the vertex's incidences in groups of QB: the records, then their corner
+                // distances, are loaded together before any is used
+                for (int qb = a.inc_ptr[i]; qb < q1; qb += QB) {
+                    int4 rec[QB];
+                    int cc[QB];
+                    T dd[QB][3];
+                    long long fx[QB];
+#pragma unroll
+                    for (int u = 0; u < QB; ++u)
+                        if (qb + u < q1) {
+                            rec[u] = a.inc_rec[qb + u];
+                            cc[u] = a.inc_corner[qb + u];
                         }
-                    } else if (kb <= rc && kb < kMaxBins) {
-                        band[S.ptr[kb] + atomicAdd(&S.fill[kb], 1)] = rec;
+#pragma unroll
+                    for (int u = 0; u < QB; ++u)
+                        if (qb + u < q1) {
+                            dd[u][0] = d[rec[u].y];
+                            dd[u][1] = d[rec[u].z];
+                            dd[u][2] = d[rec[u].w];
+                            if (pass == 0) fx[u] = a.farea_fx[rec[u].x];
+                        }
+#pragma unroll
+                    for (int u = 0; u < QB; ++u) {
+                        if (qb + u >= q1) continue;
+                        const int f = rec[u].x;
+                        const int c = cc[u];
+                        const double d0 = (double)dd[u][0], d1 = (double)dd[u][1], d2 = (double)dd[u][2];
+                        if (c >= 1 && d0 < R) continue;   // an earlier corner emits it
+                        if (c == 2 && d1 < R) continue;
+                        if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
+                        double lo = d0, hi = d0;
+                        if (d1 < lo) lo = d1;
+                        if (d1 > hi) hi = d1;
+                        if (d2 < lo) lo = d2;
+                        if (d2 > hi) hi = d2;
+                        const int kb = F.bin_of(hi);
+                        if (pass == 0) {
+                            if (hi - lo > w) longf[atomicAdd(&S.nlong, 1)] = f;
+                            if (kb <= rc && kb < kMaxBins) {
+                                atomicAdd(&S.hist[kb], (unsigned long long)fx[u]);
+                                atomicAdd(&S.ptr[kb], 1);
+                            }
+                        } else if (kb <= rc && kb < kMaxBins) {
+                            band[S.ptr[kb] + atomicAdd(&S.fill[kb], 1)] = rec[u];
+                        }
                     }
                 }
             }
