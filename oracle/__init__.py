@@ -22,3 +22,9 @@ from .heat import (  # noqa: F401
     field_eval,
     source_metrics,
 )
+from .samples import (  # noqa: F401
+    boundary_area_loss_fraction,
+    clean_vertex_samples,
+    csr,
+    vertex_samples,
+)

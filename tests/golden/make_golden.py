@@ -21,6 +21,11 @@ Fixtures:
   golden_metrics_L5.npz   same analysis outputs on a seeded folded L5 mesh (16 sources)
   golden_geometry_kat.npz lean geometry on euclid-stub and non-Lipschitz fields (L4 bumpy),
                           area/perimeter at fixed radii, per_source_geometry, NaN rules
+  golden_samples_L5.npz   sample assembly with a boundary cap on the L5 mesh: 24 sources near
+                          the boundary run through compute_all_wiring_costs(boundary_cap_fraction=0.05),
+                          their FP64 geometry records and float32 distance to boundary, the sample
+                          CSR; boundary_area_loss_fraction on an (r, d) grid; _clean_vertex_samples
+                          on crafted pair lists; the keys and dtypes save_analysis_npz writes
 """
 
 import argparse
@@ -135,6 +140,86 @@ def _analysis_fixture(ca, lg, fl, mesh, n_sources, with_stages):
     return out
 
 
+def _samples_fixture(ca, lg, mesh, n_sources, cap):
+    import io_utils as iu  # noqa: E402  (the reference's writer)
+    import tempfile
+
+    with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()):
+        an = ca.FastCorticalWiringAnalysis(mesh.vertices, mesh.faces, mesh.cortex_mask,
+                                           engine_type="consistent_heat_reference")
+    # sources spread over 0..40 mm from the boundary (in space), where the cap removes
+    # some supplementary samples and keeps others
+    Vs = an.vertices
+    bnd = an.boundary_indices
+    dist = np.min(np.linalg.norm(Vs[:, None, :] - Vs[bnd][None, :, :], axis=2), axis=1)
+    cand = np.argsort(dist, kind="stable")
+    want = np.linspace(0.0, 40.0, n_sources)
+    pick = np.unique(cand[np.searchsorted(dist[cand], want)])
+    subset = an.sub_to_orig[pick]
+    with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()), \
+            warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        an.compute_all_wiring_costs(scale=SCALES, vertex_subset=subset, n_samples_between_scales=3,
+                                    boundary_cap_fraction=cap)
+    out = dict(level=mesh.level, seed=mesh.seed, jitter=mesh.jitter, scales=np.asarray(SCALES),
+               cap=np.float64(cap), sources_sub=pick.astype(np.int64), sources_orig=subset.astype(np.int64))
+    out["field_flag"] = an.field_flag[subset]
+    out["f32_dist_to_boundary"] = an.dist_to_boundary[subset]
+    indptr, rs, as_ = [0], [], []
+    for o in subset:
+        r, a = an.get_vertex_samples(int(o))
+        rs.append(r)
+        as_.append(a)
+        indptr.append(indptr[-1] + r.size)
+    out["sample_indptr"] = np.asarray(indptr, np.int64)
+    out["sample_r"] = np.concatenate(rs).astype(np.float32)
+    out["sample_a"] = np.concatenate(as_).astype(np.float32)
+    eng = an.distance_engine._eng
+    phi = eng.compute_distance_batch(pick)
+    T = np.array(SCALES) * float(an.vertex_areas_sub.sum())
+    fr = np.array([0.25, 0.5, 0.75])
+    nF = an.faces.shape[0]
+    bufs = (np.empty(nF), np.empty(nF, np.int32), np.empty(nF, np.int32))
+    R, ER, EA = [], [], []
+    for j in range(pick.size):
+        r, p, er, ea = np.empty(12), np.empty(12), np.empty(33), np.empty(33)
+        lg.per_source_geometry(phi[j], an.faces, an._lean_area, an._lean_g11, an._lean_g12, an._lean_g22,
+                               an._lean_width, T, fr, 1e-10, 60, *bufs, r, p, er, ea)
+        R.append(r)
+        ER.append(er)
+        EA.append(ea)
+    out.update(targets=T, radii=np.array(R), extra_r=np.array(ER), extra_a=np.array(EA))
+    # boundary_area_loss_fraction on a grid, including the non-finite and degenerate cases
+    rr = np.array([0.0, -1.0, np.nan, np.inf, 1e-3, 1.0, 5.0, 10.0, 14.5, 15.2, 31.0])
+    dd = np.array([0.0, 1e-9, 0.5, 5.0, 9.99, 10.0, 10.01, 20.0, np.inf, np.nan, -1.0])
+    out["loss_r"], out["loss_d"] = np.meshgrid(rr, dd, indexing="ij")
+    out["loss"] = np.vectorize(ca.FastCorticalWiringAnalysis.boundary_area_loss_fraction)(out["loss_r"],
+                                                                                          out["loss_d"])
+    # _clean_vertex_samples on crafted lists: ties, near-duplicates, a single pair, unsorted input
+    rng = np.random.default_rng(3)
+    cases = [[(1.0, 2.0)], [(3.0, 1.0), (1.0, 2.0), (2.0, 3.0)],
+             [(1.0, 1.0), (1.0 + 1e-13, 2.0), (1.0, 3.0), (2.0, 4.0)],
+             [(5.0, 1.0), (5.0 + 3e-9, 2.0), (5.0 + 2e-8, 3.0), (10.0, 4.0)]]
+    cases.append([(float(x), float(y)) for x, y in rng.random((40, 2)) * 10])
+    cin, cout = [], []
+    for c in cases:
+        cin.append(np.asarray(c, np.float64))
+        cout.append(np.asarray(ca.FastCorticalWiringAnalysis._clean_vertex_samples(c), np.float64))
+    out["clean_in_indptr"] = np.cumsum([0] + [len(c) for c in cin]).astype(np.int64)
+    out["clean_in"] = np.concatenate(cin)
+    out["clean_out_indptr"] = np.cumsum([0] + [len(c) for c in cout]).astype(np.int64)
+    out["clean_out"] = np.concatenate(cout)
+    # what the reference's NPZ writer stores: key, dtype, shape
+    with tempfile.TemporaryDirectory() as tmp:
+        path = iu.save_analysis_npz(tmp, "a.npz", an, n_samples_between_scales=3)
+        z = np.load(path)
+        out["npz_keys"] = np.asarray(sorted(z.files))
+        out["npz_dtypes"] = np.asarray([str(z[k].dtype) for k in sorted(z.files)])
+        out["npz_ndims"] = np.asarray([z[k].ndim for k in sorted(z.files)], np.int64)
+        out["npz_schema"] = np.asarray(int(z["fastcw_output_schema_version"]))
+    return out
+
+
 def _geometry_kat(ca, lg, tk):
     V, F = tk.icosphere(4)
     with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()):
@@ -192,20 +277,31 @@ def _geometry_kat(ca, lg, tk):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default=None, help="write only this fixture (file name)")
     args = ap.parse_args()
     sys.path.insert(0, REPO)
     from fastcorticalwiring_b200.meshgen import folded_icosphere
 
     ca, de, fl, lg, tk = _ref_modules(args.reference)
     l4 = folded_icosphere(4, seed=11, jitter=0.2)
-    np.savez_compressed(os.path.join(HERE, "golden_heat_L4.npz"), **_analysis_fixture(ca, lg, fl, l4, 8, True))
     l5 = folded_icosphere(5, seed=5)
-    fx = _analysis_fixture(ca, lg, fl, l5, 16, False)
-    fx.pop("phi")  # large; the L5 fixture pins outputs, not fields
-    np.savez_compressed(os.path.join(HERE, "golden_metrics_L5.npz"), **fx)
-    np.savez_compressed(os.path.join(HERE, "golden_geometry_kat.npz"), **_geometry_kat(ca, lg, tk))
-    for n in ("golden_heat_L4.npz", "golden_metrics_L5.npz", "golden_geometry_kat.npz"):
-        print(n, os.path.getsize(os.path.join(HERE, n)))
+
+    def metrics_l5():
+        fx = _analysis_fixture(ca, lg, fl, l5, 16, False)
+        fx.pop("phi")  # large; the L5 fixture pins outputs, not fields
+        return fx
+
+    fixtures = {
+        "golden_heat_L4.npz": lambda: _analysis_fixture(ca, lg, fl, l4, 8, True),
+        "golden_metrics_L5.npz": metrics_l5,
+        "golden_geometry_kat.npz": lambda: _geometry_kat(ca, lg, tk),
+        "golden_samples_L5.npz": lambda: _samples_fixture(ca, lg, l5, 24, 0.05),
+    }
+    for name, make in fixtures.items():
+        if args.only and name != args.only:
+            continue
+        np.savez_compressed(os.path.join(HERE, name), **make())
+        print(name, os.path.getsize(os.path.join(HERE, name)))
 
 
 if __name__ == "__main__":
