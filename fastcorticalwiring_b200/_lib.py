@@ -26,6 +26,7 @@ EXPORTED = (
     "fcw_compute_distances", "fcw_compute_metrics", "fcw_compute_metrics_device", "fcw_synchronize",
     "fcw_heat_solve_device", "fcw_divergence_device", "fcw_poisson_solve_device", "fcw_field_metrics_device",
     "fcw_engine_profile", "fcw_engine_stage_times", "fcw_field_metrics_static",
+    "fcw_samples_capacity", "fcw_assemble_samples_device", "fcw_assemble_samples",
 )
 STAGES = ("heat_fwd", "heat_bwd", "divergence", "poisson_fwd", "poisson_bwd", "shift", "metrics")
 
@@ -102,6 +103,9 @@ def load():
         "fcw_poisson_solve_device": (ctypes.c_int, [P, P, P, I32, P, P]),
         "fcw_field_metrics_device": (ctypes.c_int, [P, P, P, I32, P, I32, I32, D, P, P]),
         "fcw_field_metrics_static": (ctypes.c_int, [P, P, P, I32, P, I32, I32, D, P, P]),
+        "fcw_samples_capacity": (ctypes.c_int, [I32, I32]),
+        "fcw_assemble_samples_device": (ctypes.c_int, [P, I64, I32, I32, P, D, P, P, P, P]),
+        "fcw_assemble_samples": (ctypes.c_int, [P, P, I64, I32, I32, P, D, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -138,6 +142,10 @@ def default_params(**overrides) -> FCWParams:
 
 def metrics_stride(n_targets: int, n_between: int) -> int:
     return int(load().fcw_metrics_stride(int(n_targets), int(n_between)))
+
+
+def samples_capacity(n_targets: int, n_between: int) -> int:
+    return int(load().fcw_samples_capacity(int(n_targets), int(n_between)))
 
 
 def analyze(V, F, **params):

@@ -136,6 +136,9 @@ struct fcw_engine {
     int32_t* hsrc_d = nullptr;    // staging for the host-buffer metrics API
     double* hout_d = nullptr;
     int64_t hcap_src = 0, hcap_out = 0;
+    float *hsr_d = nullptr, *hsa_d = nullptr;  // staging for the host-buffer sample assembly
+    int32_t* hcnt_d = nullptr;
+    int64_t hcap_smp = 0, hcap_cnt = 0;
     double analyze_ms = 0.0, factor_ms = 0.0;
     double lean_total = 0.0;  // sum of the lean face areas (the prefix total of a finite field)
     // stage timeline (CUDA events on the working stream), off unless enabled
@@ -1047,6 +1050,91 @@ int fcw_compute_metrics(fcw_engine* e, const int32_t* sources, int64_t n, int32_
     FCW_TRY(fcw_compute_metrics_device(e, e->hsrc_d, n, precision, targets, nt, nb, eps, e->hout_d, e->stream));
     FCW_CUDA(cudaMemcpyAsync(out_host, e->hout_d, n * stride * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
     return check_kernel_errors(e, "metrics");
+}
+
+int fcw_samples_capacity(int32_t n_targets, int32_t n_between) {
+    if (n_targets < 0 || n_between < 0) return 0;
+    return n_targets + (n_targets > 0 ? (n_targets - 1) * n_between : 0);
+}
+
+namespace {
+
+int sample_args(const double* records, int64_t n, int32_t nt, int32_t nb, const double* targets, double cap,
+                float* radii, float* areas, int32_t* count, fcw::SampleArgs& a) {
+    if (nt < 1 || nt > fcw::kMaxTargets) return fail(FCW_E_INVALID, "n_targets must be in [1, 32]");
+    if (nb < 0 || nb > fcw::kMaxBetween) return fail(FCW_E_INVALID, "n_between must be in [0, 8]");
+    if (!targets) return fail(FCW_E_INVALID, "targets is NULL");
+    if (!std::isnan(cap) && !(cap >= 0.0 && cap < 0.5))
+        return fail(FCW_E_INVALID, "boundary_cap must be in [0, 0.5), or NaN for no cap");
+    if (n < 0 || (n > 0 && (!records || !radii || !areas || !count))) return fail(FCW_E_INVALID, "NULL argument");
+    a = fcw::SampleArgs{};
+    a.n = n;
+    a.n_targets = nt;
+    a.n_between = nb;
+    a.stride = fcw_metrics_stride(nt, nb);
+    a.capacity = fcw_samples_capacity(nt, nb);
+    for (int32_t i = 0; i < nt; ++i) a.targets[i] = targets[i];
+    a.cap = cap;
+    a.records = records;
+    a.radii_out = radii;
+    a.areas_out = areas;
+    a.count_out = count;
+    return FCW_OK;
+}
+
+}  // namespace
+
+int fcw_assemble_samples_device(const double* records_dev, int64_t n, int32_t n_targets, int32_t n_between,
+                                const double* targets, double boundary_cap, float* radii_out, float* areas_out,
+                                int32_t* count_out, void* stream) {
+    fcw::SampleArgs a;
+    FCW_TRY(sample_args(records_dev, n, n_targets, n_between, targets, boundary_cap, radii_out, areas_out, count_out,
+                        a));
+    if (n == 0) return FCW_OK;
+    fcw::launch_assemble_samples(a, static_cast<cudaStream_t>(stream));
+    FCW_CUDA(cudaGetLastError());
+    return FCW_OK;
+}
+
+int fcw_assemble_samples(fcw_engine* e, const double* records, int64_t n, int32_t n_targets, int32_t n_between,
+                         const double* targets, double boundary_cap, float* radii, float* areas, int32_t* count) {
+    FCW_TRY(check_engine(e));
+    fcw::SampleArgs a;
+    FCW_TRY(sample_args(records, n, n_targets, n_between, targets, boundary_cap, radii, areas, count, a));
+    if (n == 0) return FCW_OK;
+    const int64_t stride = a.stride, cap = a.capacity;
+    if (e->hcap_out < n * stride) {
+        if (e->hout_d) e->release(e->hout_d);
+        e->hout_d = nullptr;
+        FCW_TRY(e->dalloc(&e->hout_d, (size_t)(n * stride)));
+        e->hcap_out = n * stride;
+    }
+    if (e->hcap_smp < n * cap) {
+        if (e->hsr_d) e->release(e->hsr_d);
+        if (e->hsa_d) e->release(e->hsa_d);
+        e->hsr_d = e->hsa_d = nullptr;
+        FCW_TRY(e->dalloc(&e->hsr_d, (size_t)(n * cap)));
+        FCW_TRY(e->dalloc(&e->hsa_d, (size_t)(n * cap)));
+        e->hcap_smp = n * cap;
+    }
+    if (e->hcap_cnt < n) {
+        if (e->hcnt_d) e->release(e->hcnt_d);
+        e->hcnt_d = nullptr;
+        FCW_TRY(e->dalloc(&e->hcnt_d, (size_t)n));
+        e->hcap_cnt = n;
+    }
+    FCW_CUDA(cudaMemcpyAsync(e->hout_d, records, n * stride * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    a.records = e->hout_d;
+    a.radii_out = e->hsr_d;
+    a.areas_out = e->hsa_d;
+    a.count_out = e->hcnt_d;
+    fcw::launch_assemble_samples(a, e->stream);
+    FCW_CUDA(cudaGetLastError());
+    FCW_CUDA(cudaMemcpyAsync(radii, e->hsr_d, n * cap * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    FCW_CUDA(cudaMemcpyAsync(areas, e->hsa_d, n * cap * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+    FCW_CUDA(cudaMemcpyAsync(count, e->hcnt_d, n * sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream));
+    FCW_CUDA(cudaStreamSynchronize(e->stream));
+    return FCW_OK;
 }
 
 int fcw_engine_profile(fcw_engine* e, int enable) {

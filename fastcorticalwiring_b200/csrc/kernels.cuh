@@ -157,6 +157,20 @@ struct MetricArgs {
     int32_t* near_count = nullptr;      // K
 };
 constexpr int kStatVTile = 256;   // vertices per shift-statistics CTA
+
+// ---- per-source sample assembly (samples.cu) ----
+constexpr int kMaxSamples = kMaxTargets + (kMaxTargets - 1) * kMaxBetween;
+struct SampleArgs {
+    int64_t n = 0;                    // sources (records)
+    int32_t n_targets = 0, n_between = 0, stride = 0, capacity = 0;
+    double targets[kMaxTargets];
+    double cap = 0.0;                 // boundary cap on the clipped disc fraction; NaN: none
+    const double* records = nullptr;  // n x stride (fcw_compute_metrics layout)
+    float* radii_out = nullptr;       // n x capacity
+    float* areas_out = nullptr;       // n x capacity
+    int32_t* count_out = nullptr;     // n
+};
+void launch_assemble_samples(const SampleArgs& a, cudaStream_t st);
 // phi (n x K) -> dT (K x n) with phi[source] subtracted, plus per-tile health/MSD
 // partials and the per-source near-vertex lists.
 template <typename Tin, typename Tout>

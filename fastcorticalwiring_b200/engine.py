@@ -105,6 +105,24 @@ class HeatEngine:
             _lib.ptr(t), t.size, int(n_between), float(eps), ctypes.c_void_p(out_dev.data_ptr()),
             ctypes.c_void_p(stream)))
 
+    def assemble_samples(self, records, targets, n_between=3, boundary_cap=None):
+        """Cleaned (radius, area) samples of metric records (core_analysis.py:1599-1611).
+
+        Returns (radii, areas, counts): float32 rows of fcw_samples_capacity entries, of
+        which counts[k] are used. boundary_cap: None, or the cap in [0, 0.5).
+        """
+        rec = np.ascontiguousarray(records, dtype=np.float64)
+        t = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1)
+        n = rec.shape[0]
+        cap = _lib.samples_capacity(t.size, n_between)
+        radii = np.empty((n, cap), dtype=np.float32)
+        areas = np.empty((n, cap), dtype=np.float32)
+        counts = np.empty(n, dtype=np.int32)
+        c = float("nan") if boundary_cap is None else float(boundary_cap)
+        _lib.check(_lib.load().fcw_assemble_samples(self.handle, _lib.ptr(rec), n, t.size, int(n_between), _lib.ptr(t),
+                                                    c, _lib.ptr(radii), _lib.ptr(areas), _lib.ptr(counts)))
+        return radii, areas, counts
+
     def profile(self, enable=True) -> None:
         """Turn the per-stage CUDA-event timeline on/off (and reset it)."""
         _lib.check(_lib.load().fcw_engine_profile(self.handle, int(bool(enable))))

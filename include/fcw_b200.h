@@ -146,6 +146,25 @@ int fcw_compute_metrics_device(fcw_engine* e, const int32_t* sources_dev, int64_
                                const double* targets_host, int32_t n_targets, int32_t n_between,
                                double eps, double* out_dev, void* stream);
 
+/* Cleaned (radius, area) samples of metric records (the fcw_compute_metrics
+ * layout, n records of fcw_metrics_stride(nt, nb) doubles). Per healthy source:
+ * the finite solved radii paired with their target areas, then the finite
+ * supplementary samples, less those whose disc loses more than boundary_cap of
+ * its area to a straight boundary at the record's distance to boundary rounded
+ * to float32 (NaN: no cap; else in [0, 0.5)); stably sorted by radius, radii
+ * within max(1e-12, 1e-9 * span) of their predecessor dropped, stored as float32
+ * in rows of fcw_samples_capacity(nt, nb) with count_out[k] used. Flagged fields
+ * get count 0. Replaces core_analysis.py:1599-1611 with boundary_area_loss_fraction
+ * (:759-777) and _clean_vertex_samples (:1424-1439); the CSR over vertices
+ * (:1619-1632) is the caller's concatenation of the rows. */
+int fcw_samples_capacity(int32_t n_targets, int32_t n_between);
+int fcw_assemble_samples_device(const double* records_dev, int64_t n, int32_t n_targets, int32_t n_between,
+                                const double* targets, double boundary_cap, float* radii_out, float* areas_out,
+                                int32_t* count_out, void* stream);
+/* The same on host buffers, staged through the engine's device buffers. */
+int fcw_assemble_samples(fcw_engine* e, const double* records, int64_t n, int32_t n_targets, int32_t n_between,
+                         const double* targets, double boundary_cap, float* radii, float* areas, int32_t* count);
+
 /* Stage timeline: enable (1) / disable (0) CUDA-event marks between pipeline
  * stages on the working stream and reset the accumulated times and launch count. */
 int fcw_engine_profile(fcw_engine* e, int enable);
