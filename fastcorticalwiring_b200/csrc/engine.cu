@@ -147,21 +147,31 @@ struct fcw_engine {
     double stage_ms[FCW_N_STAGES] = {0};
     int64_t launches = 0;
 
+    // Device memory is stream-ordered (the device's default pool): freeing it
+    // waits for this engine's streams only, never for other engines' work, so
+    // engines can come and go while others run (the serving loop relies on it).
     template <typename T>
     int dalloc(T** p, size_t count) {
         *p = nullptr;
         if (count == 0) count = 1;
         void* q = nullptr;
-        cudaError_t e = cudaMalloc(&q, count * sizeof(T));
+        cudaError_t e = cudaMallocAsync(&q, count * sizeof(T), stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // usable from any stream from here on
         if (e != cudaSuccess) {
             cudaGetLastError();
-            return fail(FCW_E_NOMEM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed: " +
+            return fail(FCW_E_NOMEM, "allocation of " + std::to_string(count * sizeof(T)) + " bytes failed: " +
                                          cudaGetErrorString(e));
         }
         allocs.push_back(q);
         bytes += (int64_t)(count * sizeof(T));
         *p = static_cast<T*>(q);
         return FCW_OK;
+    }
+    // Waits for all of this engine's streams (the work that may still read its buffers).
+    void sync_streams() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& w : pool)
+            if (w.stream) cudaStreamSynchronize(w.stream);
     }
     template <typename T>
     int upload(T** p, const std::vector<T>& h) {
@@ -172,12 +182,16 @@ struct fcw_engine {
     void release(void* p) {
         for (size_t i = 0; i < allocs.size(); ++i)
             if (allocs[i] == p) {
-                cudaFree(p);
+                sync_streams();
+                cudaFreeAsync(p, stream);
                 allocs.erase(allocs.begin() + (long)i);
                 return;
             }
     }
     ~fcw_engine() {
+        sync_streams();
+        for (void* p : allocs) cudaFreeAsync(p, stream);
+        if (stream) cudaStreamSynchronize(stream);
         for (auto& w : pool) {
             for (auto& m : w.marks) cudaEventDestroy(m.second);
             if (w.done) cudaEventDestroy(w.done);
@@ -185,7 +199,6 @@ struct fcw_engine {
         }
         if (ev_in) cudaEventDestroy(ev_in);
         for (cudaEvent_t ev : event_pool) cudaEventDestroy(ev);
-        for (void* p : allocs) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
     }
 };
