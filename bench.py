@@ -475,6 +475,60 @@ def _fp64_forms_and_errors(eng, pm, targets, stream, args, dev):
     }
 
 
+def run_serving(args):
+    """The serving stream (hemisphere jobs of mixed sizes arriving as a Poisson process).
+
+    Jobs: 40% order-5, 40% order-6 (jitter 0.2), 20% order-7 folded icospheres, each with
+    its own folding seed and a medial-wall cap of 8-12% of the vertices, all cortical
+    sources per job. For each arrival rate the server admits jobs against the HBM
+    budget and reports p50/p99 job latency (arrival to results on the host) and the
+    stream's sources/s (all sources over the time from the first arrival to the last
+    result). Meshes are generated before the stream starts.
+    """
+    import torch
+
+    from fastcorticalwiring_b200 import serving
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    rng = np.random.default_rng(args.seed)
+    n = args.serving_jobs
+    levels = rng.choice([5, 6, 7], size=n, p=[0.4, 0.4, 0.2])
+    jobs = []
+    for i, lv in enumerate(levels):
+        m = folded_icosphere(int(lv), seed=1000 + i, jitter=0.2 if lv == 6 else 0.0,
+                             cap_fraction=float(rng.uniform(0.08, 0.12)))
+        jobs.append(serving.Job(f"job{i}-L{lv}", m.vertices, m.faces, m.cortex_mask, precision=args.precision))
+    torch.cuda.set_device(args.device)
+    rows = []
+    for rate in [float(x) for x in args.serving_rates.split(",")]:
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+        arrivals -= arrivals[0]
+        srv = serving.Server(hbm_budget_bytes=args.hbm_budget_gb * 1e9, device=args.device,
+                             engine_params=dict(block_k=args.block_k, pipeline_depth=2))
+        try:
+            t0 = time.perf_counter()
+            res = srv.run(list(zip(arrivals.tolist(), jobs)))
+            span = time.perf_counter() - t0
+        finally:
+            srv.close()
+        lat = serving.latency_summary(res)
+        total = sum(r.sources.size for r in res.values())
+        by_level = {}
+        for r in res.values():
+            by_level.setdefault(r.job_id.split("-")[1], []).append(r.latency_s)
+        rows.append({"rate_jobs_per_s": rate, "sources_per_s": total / span, "sources": int(total),
+                     "span_s": span, **lat,
+                     "p50_s_by_level": {k: float(np.percentile(v, 50)) for k, v in sorted(by_level.items())},
+                     "peak_device_bytes_per_job": int(max(r.device_bytes for r in res.values()))})
+    line = {"metric": "serving: job p50/p99 latency and sources/s", "unit": "s / sources/s", "n_gpus": 1,
+            "jobs": n, "mix": {"L5": int((levels == 5).sum()), "L6": int((levels == 6).sum()),
+                               "L7": int((levels == 7).sum())},
+            "hbm_budget_gb": args.hbm_budget_gb, "precision": args.precision, "block_k": args.block_k,
+            "data": "synthetic", "rates": rows}
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -493,7 +547,13 @@ def main(argv=None):
     ap.add_argument("--fp64-sample", type=int, default=16)
     ap.add_argument("--ref-sources-per-core", type=int, default=2)
     ap.add_argument("--quick", action="store_true", help="skip the FP64 forms and the accuracy check")
+    ap.add_argument("--serving", action="store_true", help="run the serving stream instead (own JSON line)")
+    ap.add_argument("--serving-jobs", type=int, default=64)
+    ap.add_argument("--serving-rates", default="0.5,2,8", help="Poisson arrival rates, jobs/s")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     args = ap.parse_args(argv)
+    if args.serving:
+        return run_serving(args)
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.impl == "reference":

@@ -106,15 +106,27 @@ def vertex_areas(nv, F, face_area):
     return a
 
 
-def boundary_vertices(F):
-    """Vertices on free edges (edges used by exactly one face), sorted (core_analysis.py:651-665)."""
+def _edge_keys(F):
+    """Undirected edges of the faces as sorted int64 keys lo * n + hi (n = max vertex id + 1)."""
     e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]], axis=0).astype(np.int64)
     e.sort(axis=1)
-    ue, cnt = np.unique(e, axis=0, return_counts=True)
-    be = ue[cnt == 1]
+    n = int(F.max()) + 1 if F.size else 1
+    return np.sort(e[:, 0] * n + e[:, 1]), n
+
+
+def boundary_vertices(F):
+    """Vertices on free edges (edges used by exactly one face), sorted (core_analysis.py:651-665)."""
+    key, n = _edge_keys(F)
+    if key.size == 0:
+        return np.empty(0, dtype=np.int32)
+    first = np.ones(key.size, dtype=bool)
+    first[1:] = key[1:] != key[:-1]
+    starts = np.flatnonzero(first)
+    cnt = np.diff(np.append(starts, key.size))
+    be = key[starts[cnt == 1]]
     if be.size == 0:
         return np.empty(0, dtype=np.int32)
-    return np.unique(be.reshape(-1)).astype(np.int32)
+    return np.unique(np.concatenate([be // n, be % n])).astype(np.int32)
 
 
 def mean_edge_length(V, F):
@@ -129,39 +141,60 @@ def vertex_adjacency_csr(nv, F):
     """Sorted neighbour lists as CSR (indptr int64, indices int32)."""
     e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]],
                         F[:, [1, 0]], F[:, [2, 1]], F[:, [0, 2]]], axis=0).astype(np.int64)
-    key = np.unique(e[:, 0] * nv + e[:, 1])
+    key = np.sort(e[:, 0] * nv + e[:, 1])
+    if key.size:
+        keep = np.ones(key.size, dtype=bool)
+        keep[1:] = key[1:] != key[:-1]
+        key = key[keep]
     rows = key // nv
     cols = (key % nv).astype(np.int32)
     indptr = np.zeros(nv + 1, dtype=np.int64)
-    np.add.at(indptr, rows + 1, 1)
-    np.cumsum(indptr, out=indptr)
+    indptr[1:] = np.cumsum(np.bincount(rows, minlength=nv))
     return indptr, cols
 
 
 def bfs_order(nv, F, start=0):
-    """BFS over all components, neighbours in ascending order (core_analysis.py:1385-1417)."""
+    """BFS over all components, neighbours in ascending order (core_analysis.py:1385-1417).
+
+    Level by level: the next frontier is the frontier's neighbour lists, in frontier
+    order, unvisited, each vertex at its first appearance -- exactly the order a FIFO
+    queue visits them in.
+    """
     indptr, nbr = vertex_adjacency_csr(nv, F)
     visited = np.zeros(nv, dtype=bool)
     order = []
+    deg = np.diff(indptr)
 
     def run(s):
-        q = deque([s])
         visited[s] = True
-        while q:
-            v = q.popleft()
-            order.append(v)
-            for w in nbr[indptr[v]:indptr[v + 1]]:
-                if not visited[w]:
-                    visited[w] = True
-                    q.append(int(w))
+        front = np.array([s], dtype=np.int64)
+        while front.size:
+            order.append(front)
+            d = deg[front]
+            tot = int(d.sum())
+            if tot == 0:
+                break
+            # positions of the frontier's neighbour lists, concatenated in frontier order
+            off = np.repeat(indptr[front] - np.cumsum(d) + d, d) + np.arange(tot)
+            cand = nbr[off].astype(np.int64)
+            cand = cand[~visited[cand]]
+            if cand.size == 0:
+                break
+            _, first = np.unique(cand, return_index=True)
+            front = cand[np.sort(first)]
+            visited[front] = True
 
     s0 = int(start) if 0 <= int(start) < nv else 0
     if nv:
         run(s0)
-    for v in range(nv):
-        if not visited[v]:
-            run(v)
-    return np.asarray(order, dtype=np.int64)
+        nxt = 0
+        while True:
+            rest = np.flatnonzero(~visited[nxt:])
+            if rest.size == 0:
+                break
+            nxt += int(rest[0])
+            run(nxt)
+    return np.concatenate(order) if order else np.empty(0, dtype=np.int64)
 
 
 def lean_face_metric(V, F):

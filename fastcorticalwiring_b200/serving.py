@@ -1,12 +1,14 @@
 """A request loop for hemisphere jobs on one GPU: continuous batching under an HBM budget.
 
-Jobs (a cortical mesh, its scales, the sources to run) arrive at any time. A
-builder thread admits them in arrival order when their device memory fits the
-budget, prepares the mesh and factors it; the factors and the job's
+Jobs (a cortical mesh, its scales, the sources to run) arrive at any time. Builder
+threads admit them when their device memory fits the budget (in arrival order,
+except that a job that fits may pass a head job waiting for memory a bounded
+number of times), prepare the mesh and factor it; the factors and the job's
 right-hand-side blocks stay resident until the job is done. The dispatch loop
-keeps every admitted job's next chunk of source blocks enqueued on the job's
-own stream, so the blocks of all admitted jobs overlap on the device, and a job
-that arrives while others run starts as soon as memory frees up. Each job
+keeps the next chunk of source blocks of the few admitted jobs with the least
+work left enqueued on each job's own stream, so their blocks overlap on the
+device, and a job that arrives while others run starts as soon as memory frees
+up and it is among the shortest. Each job
 reports its latency (arrival to results on the host) beside the whole stream's
 throughput.
 
@@ -102,25 +104,33 @@ def estimate_device_bytes(n_vertices: int, n_faces: int, block_k: int, pipeline_
 class Server:
     """Continuous batching of hemisphere jobs on one GPU under an HBM budget (bytes)."""
 
-    def __init__(self, hbm_budget_bytes=150e9, device=0, chunk_blocks=8, engine_params=None):
+    def __init__(self, hbm_budget_bytes=150e9, device=0, chunk_blocks=8, engine_params=None, builders=4,
+                 max_running=3, max_bypass=8):
         import torch
 
         self.torch = torch
         self.device = int(device)
         self.budget = int(hbm_budget_bytes)
         self.chunk_blocks = int(chunk_blocks)
+        self.max_running = max(1, int(max_running))  # jobs with source blocks on the device at once
+        self.max_bypass = int(max_bypass)  # admissions that may pass a head job waiting for memory
         self.params = dict(block_k=1024, pipeline_depth=2)
         self.params.update(engine_params or {})
         self._cv = threading.Condition()
         self._pending: deque[_Pending] = deque()
         self._ready: deque[_Active] = deque()
         self._reserved = 0
+        self._bypassed = 0
         self._n_open = 0  # submitted and not finished
         self._closed = False
         self._error: BaseException | None = None
         self.results: dict[str, JobResult] = {}
-        self._builder = threading.Thread(target=self._build_loop, name="fcw-serving-builder", daemon=True)
-        self._builder.start()
+        # builders prepare and factor admitted jobs in parallel (mesh preparation and
+        # the symbolic analysis run on the host); admission itself stays in arrival order
+        self._builders = [threading.Thread(target=self._build_loop, name=f"fcw-serving-builder-{i}", daemon=True)
+                          for i in range(max(1, int(builders)))]
+        for t in self._builders:
+            t.start()
 
     # -- public ----------------------------------------------------------------
     def submit(self, job: Job) -> None:
@@ -154,17 +164,19 @@ class Server:
                     break
             progressed = False
             for a in list(active):
-                if a.event is not None and not a.event.query():
-                    continue
-                if a.event is not None:
+                if a.event is not None and a.event.query():
                     a.event = None
                     progressed = True
-                if a.next0 >= a.sources.size:
-                    self._finish(a)
-                    active.remove(a)
-                    continue
-                self._enqueue(a)
-                progressed = True
+                    if a.next0 >= a.sources.size:
+                        self._finish(a)
+                        active.remove(a)
+            # shortest remaining work first: the jobs with the fewest sources left keep a
+            # chunk on the device; the others stay resident and wait their turn
+            active.sort(key=lambda x: x.sources.size - x.next0)
+            for a in active[:self.max_running]:
+                if a.event is None and a.next0 < a.sources.size:
+                    self._enqueue(a)
+                    progressed = True
             if not progressed:
                 time.sleep(poll_s)
         return self.results
@@ -173,7 +185,8 @@ class Server:
         with self._cv:
             self._closed = True
             self._cv.notify_all()
-        self._builder.join(timeout=60)
+        for t in self._builders:
+            t.join(timeout=60)
 
     # -- internals -------------------------------------------------------------
     def _enqueue(self, a: _Active) -> None:
@@ -207,25 +220,16 @@ class Server:
         torch.cuda.set_device(self.device)
         while True:
             with self._cv:
-                while not self._closed and not self._pending:
+                # admission in arrival order: take the head job once it fits the budget
+                # (or once nothing else is resident)
+                while True:
+                    if self._closed:
+                        return
+                    p = self._pick()
+                    if p is not None:
+                        self._reserved += p.estimate
+                        break
                     self._cv.wait()
-                if self._closed:
-                    return
-                p = self._pending[0]
-                job = p.job
-                nv = int(np.count_nonzero(job.cortex_mask))
-                nf = 2 * nv
-                nsrc = nv if job.sources is None else int(np.asarray(job.sources).size)
-                stride = _stride(len(job.scales), job.n_between)
-                p.estimate = estimate_device_bytes(nv, nf, self.params["block_k"], self.params["pipeline_depth"],
-                                                   nsrc, stride)
-                # admission in arrival order: wait until the head job fits (or nothing else is resident)
-                while not self._closed and self._reserved > 0 and self._reserved + p.estimate > self.budget:
-                    self._cv.wait()
-                if self._closed:
-                    return
-                self._pending.popleft()
-                self._reserved += p.estimate
             try:
                 act = self._admit(p)
             except BaseException as exc:  # surfaced by run()
@@ -241,6 +245,35 @@ class Server:
                 self._reserved += act.reserved - p.estimate
                 self._ready.append(act)
                 self._cv.notify_all()
+
+    def _estimate(self, p: _Pending) -> int:
+        if not p.estimate:
+            job = p.job
+            nv = int(np.count_nonzero(job.cortex_mask))
+            nsrc = nv if job.sources is None else int(np.asarray(job.sources).size)
+            p.estimate = estimate_device_bytes(nv, 2 * nv, self.params["block_k"], self.params["pipeline_depth"],
+                                               nsrc, _stride(len(job.scales), job.n_between))
+        return p.estimate
+
+    def _pick(self):
+        """The next job to admit (caller holds the lock): the head of the queue if it fits
+        the budget (or nothing is resident); else the first later job that fits, while the
+        head has been passed fewer than max_bypass times."""
+        if not self._pending:
+            return None
+        head = self._pending[0]
+        if self._reserved == 0 or self._reserved + self._estimate(head) <= self.budget:
+            self._bypassed = 0
+            return self._pending.popleft()
+        if self._bypassed >= self.max_bypass:
+            return None
+        for i in range(1, len(self._pending)):
+            q = self._pending[i]
+            if self._reserved + self._estimate(q) <= self.budget:
+                del self._pending[i]
+                self._bypassed += 1
+                return q
+        return None
 
     def _admit(self, p: _Pending) -> _Active:
         torch = self.torch
