@@ -397,7 +397,8 @@ def run_gpu(args):
             "clocks": clk,
             "engine": {"factor_ms": info["factor_ms"], "analyze_ms": info["analyze_ms"], "build_s": build_s,
                        "n_supernodes": info["n_supernodes"], "n_levels": info["n_levels"],
-                       "nnz_factor": info["nnz_factor"], "device_bytes": info["device_bytes"]},
+                       "nnz_factor": info["nnz_factor"], "device_bytes": info["device_bytes"],
+                       "pipeline_depth_held": info["pipeline_depth"]},
         }
         line.update(extra)
         if cpu is not None:

@@ -55,6 +55,7 @@ class FCWInfo(ctypes.Structure):
         ("bin_width", ctypes.c_double), ("health_h", ctypes.c_double), ("total_vertex_area", ctypes.c_double),
         ("analyze_ms", ctypes.c_double), ("factor_ms", ctypes.c_double), ("flops_factor", ctypes.c_double),
         ("device_bytes", ctypes.c_int64),
+        ("pipeline_depth", ctypes.c_int32), ("block_k", ctypes.c_int32),
     ]
 
     def as_dict(self):

@@ -103,7 +103,7 @@ struct fcw_engine {
     double t_coef = 0.0, t = 0.0;
     int32_t ground_new = -1;
     cudaStream_t stream = nullptr;
-    std::vector<void*> allocs;
+    std::vector<std::pair<void*, size_t>> allocs;  // device allocations and their sizes
     int64_t bytes = 0;
     fcw::DevPlan plan;
     std::vector<int32_t> level_tiles;
@@ -162,7 +162,7 @@ struct fcw_engine {
             return fail(FCW_E_NOMEM, "allocation of " + std::to_string(count * sizeof(T)) + " bytes failed: " +
                                          cudaGetErrorString(e));
         }
-        allocs.push_back(q);
+        allocs.emplace_back(q, count * sizeof(T));
         bytes += (int64_t)(count * sizeof(T));
         *p = static_cast<T*>(q);
         return FCW_OK;
@@ -181,16 +181,17 @@ struct fcw_engine {
     }
     void release(void* p) {
         for (size_t i = 0; i < allocs.size(); ++i)
-            if (allocs[i] == p) {
+            if (allocs[i].first == p) {
                 sync_streams();
                 cudaFreeAsync(p, stream);
+                bytes -= (int64_t)allocs[i].second;
                 allocs.erase(allocs.begin() + (long)i);
                 return;
             }
     }
     ~fcw_engine() {
         sync_streams();
-        for (void* p : allocs) cudaFreeAsync(p, stream);
+        for (auto& a : allocs) cudaFreeAsync(a.first, stream);
         if (stream) cudaStreamSynchronize(stream);
         for (auto& w : pool) {
             for (auto& m : w.marks) cudaEventDestroy(m.second);
@@ -575,12 +576,10 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
         FCW_CUDA(cudaStreamSynchronize(e->stream));
         e->release(val_tmp);
         e->release(inv_tmp);
-        e->bytes -= (int64_t)(S.nnz_factor + S.n_inv) * 8;
     }
     FCW_CUDA(cudaStreamSynchronize(e->stream));
     e->release(upd);
     e->release(aval_d);
-    e->bytes -= (int64_t)(std::max<int64_t>(S.n_upd, 1) + std::max<int64_t>(S.nnz_lower_a, 1)) * 8;
     e->factor_ms = now_ms() - t0;
     return FCW_OK;
 }
@@ -625,8 +624,28 @@ int ensure_one(fcw_engine* e, Workspace& w, int32_t K, int32_t stride) {
 }
 
 // Every workspace of the pool holds at least K columns and `stride` output doubles per column.
+// If the device cannot hold another workspace, the pool keeps the ones that fit (at least
+// one): fewer blocks are in flight, nothing else changes.
 int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
-    for (auto& w : e->pool) FCW_TRY(ensure_one(e, w, K, stride));
+    for (size_t i = 0; i < e->pool.size(); ++i) {
+        const int rc = ensure_one(e, e->pool[i], K, stride);
+        if (rc == FCW_OK) continue;
+        if (i == 0 || rc != FCW_E_NOMEM) return rc;
+        e->sync_streams();
+        for (size_t j = i; j < e->pool.size(); ++j) {
+            Workspace& w = e->pool[j];
+            void* bufs[] = {w.Bh, w.Bp64, w.Y, w.dT64, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
+                            w.counters, w.partials, w.near_list, w.near_count};
+            for (void* p : bufs)
+                if (p) e->release(p);
+            for (auto& m : w.marks) cudaEventDestroy(m.second);
+            if (w.done) cudaEventDestroy(w.done);
+            if (w.stream) cudaStreamDestroy(w.stream);
+        }
+        e->pool.resize(i);
+        e->cur_ws = 0;
+        return FCW_OK;
+    }
     return FCW_OK;
 }
 
@@ -940,6 +959,8 @@ int fcw_engine_info(const fcw_engine* e, fcw_info* info) {
     info->factor_ms = e->factor_ms;
     info->flops_factor = S.flops_factor;
     info->device_bytes = e->bytes;
+    info->pipeline_depth = (int32_t)e->pool.size();
+    info->block_k = e->prm.block_k;
     return FCW_OK;
 }
 

@@ -63,6 +63,8 @@ typedef struct fcw_info {
     double total_vertex_area;   /* sum of barycentric vertex areas */
     double analyze_ms, factor_ms, flops_factor;
     int64_t device_bytes;       /* device memory held by the engine */
+    int32_t pipeline_depth;     /* blocks in flight the device holds workspaces for (<= params) */
+    int32_t block_k;            /* sources per block */
 } fcw_info;
 
 /* Per-source metric record: FCW_M_* offsets, then radii[nt], perimeters[nt],
