@@ -275,6 +275,15 @@ def run_gpu(args):
     torch.cuda.set_device(dev)
     _, pm = _mesh(args.workload, args.seed)
     targets = pm.targets(M.RUNNER_SCALES)
+    tuned = None
+    if args.autotune:
+        from fastcorticalwiring_b200.autotune import autotune
+
+        t0 = time.perf_counter()
+        best, trials = autotune(pm, precision=args.precision, device=dev)
+        args.block_k, args.pipeline_depth = best["block_k"], best["pipeline_depth"]
+        tuned = {"chosen": best, "tune_s": time.perf_counter() - t0,
+                 "trials": [{k: (round(v, 1) if isinstance(v, float) else v) for k, v in t.items()} for t in trials]}
     t0 = time.perf_counter()
     eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k, pipeline_depth=args.pipeline_depth)
     build_s = time.perf_counter() - t0
@@ -401,6 +410,8 @@ def run_gpu(args):
                        "pipeline_depth_held": info["pipeline_depth"]},
         }
         line.update(extra)
+        if tuned is not None:
+            line["autotune"] = tuned
         if cpu is not None:
             p, q, n = cpu
             try:
@@ -548,6 +559,7 @@ def main(argv=None):
     ap.add_argument("--fp64-sample", type=int, default=16)
     ap.add_argument("--ref-sources-per-core", type=int, default=2)
     ap.add_argument("--quick", action="store_true", help="skip the FP64 forms and the accuracy check")
+    ap.add_argument("--autotune", action="store_true", help="choose block size and depth on the mesh first")
     ap.add_argument("--serving", action="store_true", help="run the serving stream instead (own JSON line)")
     ap.add_argument("--serving-jobs", type=int, default=64)
     ap.add_argument("--serving-rates", default="0.5,2,8", help="Poisson arrival rates, jobs/s")
