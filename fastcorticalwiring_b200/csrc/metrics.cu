@@ -209,6 +209,11 @@ __device__ __forceinline__ double warp_sum(double v) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
+// Threads per source CTA: four CTAs share an SM, so one source's barrier waits
+// (uneven near-vertex walks, idle warps in the last round of targets) overlap
+// with the other sources' work.
+constexpr int kMetricThreads = 256;
+
 struct SrcShared {
     union {
         unsigned long long hist[kMaxBins + 1];  // face areas per bin, fixed point (order-free sums)
@@ -390,7 +395,7 @@ struct Field {
 //      rc grows (up to every bin, scanning all vertices) and step 2 repeats;
 //   3. one warp per target: bracket + safeguarded Newton + perimeter; then the samples.
 template <typename T>
-__global__ void __launch_bounds__(512, 2) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
+__global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
     __shared__ SrcShared S;
     const int k = blockIdx.x;
     const int src = a.src[k];
@@ -668,7 +673,7 @@ void launch_shift_stats(const MetricArgs& a, int32_t K, const Tin* phi, Tout* dT
 template <typename T>
 void launch_source_metrics(const MetricArgs& a, const T* dT, cudaStream_t st) {
     if (a.nsrc <= 0) return;
-    k_source_metrics<T><<<a.nsrc, 512, 0, st>>>(a, dT);
+    k_source_metrics<T><<<a.nsrc, kMetricThreads, 0, st>>>(a, dT);
 }
 
 template void launch_shift_transpose<double, double>(int32_t, int32_t, const double*, const int32_t*, double*,
