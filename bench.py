@@ -175,7 +175,7 @@ def _config(args, pm):
     return {"workload": f"{args.workload} folded icosphere, {pm.n_vertices} cortical sources, "
                         f"{pm.n_faces} faces, t=(0.7 mm)^2, 12 scales + {N_BETWEEN} samples between",
             "batch_sources_per_step": args.batch, "block_k": args.block_k, "precision": args.precision,
-            "pipeline_depth": args.pipeline_depth,
+            "pipeline_depth": args.pipeline_depth, "leaf_size": args.leaf_size, "relax": args.relax,
             "parallelism": f"replicas{args.gpus}", "l2": "inputs larger than L2 (n x K RHS blocks > 126 MB)"}
 
 
@@ -285,7 +285,8 @@ def run_gpu(args):
         tuned = {"chosen": best, "tune_s": time.perf_counter() - t0,
                  "trials": [{k: (round(v, 1) if isinstance(v, float) else v) for k, v in t.items()} for t in trials]}
     t0 = time.perf_counter()
-    eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k, pipeline_depth=args.pipeline_depth)
+    eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k, pipeline_depth=args.pipeline_depth,
+                       leaf_size=args.leaf_size, relax=args.relax)
     build_s = time.perf_counter() - t0
     info = eng.info()
 
@@ -554,6 +555,8 @@ def main(argv=None):
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--pipeline-depth", type=int, default=3, help="blocks in flight on separate streams")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--leaf-size", type=int, default=64, help="nested-dissection leaf size")
+    ap.add_argument("--relax", type=int, default=64, help="relaxed supernode amalgamation (columns)")
     ap.add_argument("--cpu-sample", type=int, default=24, help="sources timed on the CPU oracle (0 = skip)")
     ap.add_argument("--cpu-timeout", type=float, default=600.0)
     ap.add_argument("--fp64-sample", type=int, default=16)

@@ -835,7 +835,7 @@ void fcw_default_params(fcw_params* p) {
     p->block_k = 1024;
     p->leaf_size = 64;
     p->max_width = 64;
-    p->relax = 32;
+    p->relax = 64;
     p->build_mixed = 1;
     p->device = 0;
     p->pipeline_depth = 3;

@@ -92,7 +92,7 @@ enum {
     FCW_N_STAGES = 7
 };
 
-/* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 32, mixed on, 2 blocks in flight). */
+/* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 64, mixed on, 3 blocks in flight). */
 void fcw_default_params(fcw_params* p);
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between);
