@@ -559,6 +559,7 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
             fcw::launch_factor_front(e->plan, l0, cnt, val, inv, upd, e->err_d, e->stream);
             fcw::launch_factor_update(e->plan, l0, cnt, e->level_tiles[l], val, upd, e->stream);
         }
+        fcw::launch_panel_inverse(e->plan, val, inv, e->stream);
         FCW_CUDA(cudaGetLastError());
         return check_kernel_errors(e, what);
     };

@@ -8,7 +8,10 @@
 // its children's update matrices (extend-add, children in a fixed order, so the
 // result is deterministic), factors the dense ns x ns block in shared memory,
 // inverts it, forms L21 = F21 L11^{-T}, and a second launch per level subtracts
-// L21 L21^T from U_s in 32 x 32 tiles.
+// L21 L21^T from U_s in 32 x 32 tiles. Once every level is factored, a last
+// launch replaces each L21 by Q = L21 L11^{-1}: with it the solves form update
+// rows (forward) and corrections (backward) straight from the right-hand side,
+// without waiting for X_s = L11^{-1} (...).
 #include "kernels.cuh"
 
 namespace fcw {
@@ -172,6 +175,39 @@ __global__ void __launch_bounds__(256) k_factor_update(DevPlan p, int32_t l0, co
     }
 }
 
+// Row p of the panel becomes sum_{k >= j} L21[p][k] Li[k][j] (Li = L11^{-1}, lower).
+__global__ void __launch_bounds__(256) k_panel_inverse(DevPlan p, double* __restrict__ val,
+                                                       const double* __restrict__ inv) {
+    __shared__ double Li[kMaxWidth * kLd];
+    const int s = blockIdx.x;
+    const int ns = p.sn_c0[s + 1] - p.sn_c0[s];
+    const int m = p.sn_m[s];
+    if (m == ns || ns > kMaxWidth) return;
+    const double* I = inv + p.sn_invptr[s];
+    const int tid = threadIdx.x;
+    for (int e = tid; e < ns * ns; e += blockDim.x) {
+        const int i = e / ns, j = e - i * ns;
+        Li[i * kLd + j] = I[e];
+    }
+    __syncthreads();
+    double* P = val + p.sn_valptr[s];
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    for (int row = ns + warp; row < m; row += nwarps) {
+        double* Rw = P + (int64_t)row * ns;
+        const double f0 = lane < ns ? Rw[lane] : 0.0;
+        const double f1 = lane + 32 < ns ? Rw[lane + 32] : 0.0;
+        double o0 = 0.0, o1 = 0.0;
+        for (int k = 0; k < ns; ++k) {
+            const double fk = __shfl_sync(0xffffffffu, k < 32 ? f0 : f1, k & 31);
+            if (lane <= k && lane < ns) o0 += fk * Li[k * kLd + lane];
+            if (lane + 32 <= k && lane + 32 < ns) o1 += fk * Li[k * kLd + lane + 32];
+        }
+        __syncwarp();
+        if (lane < ns) Rw[lane] = o0;
+        if (lane + 32 < ns) Rw[lane + 32] = o1;
+    }
+}
+
 }  // namespace
 
 cudaError_t configure_kernels() {
@@ -198,6 +234,11 @@ void launch_factor_front(const DevPlan& p, int32_t l0, int32_t count, double* va
     if (count <= 0) return;
     const size_t smem = 2 * kMaxWidth * kLd * sizeof(double);
     k_factor_front<<<count, 256, smem, st>>>(p, l0, val, inv, upd, err);
+}
+
+void launch_panel_inverse(const DevPlan& p, double* val, const double* inv, cudaStream_t st) {
+    if (p.nsuper <= 0) return;
+    k_panel_inverse<<<p.nsuper, 256, 0, st>>>(p, val, inv);
 }
 
 void launch_factor_update(const DevPlan& p, int32_t l0, int32_t count, int32_t max_tiles, const double* val,

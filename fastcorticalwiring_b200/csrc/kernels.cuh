@@ -52,6 +52,8 @@ void launch_factor_front(const DevPlan& p, int32_t l0, int32_t count, double* va
 void launch_factor_update(const DevPlan& p, int32_t l0, int32_t count, int32_t max_tiles, const double* val,
                           double* upd, cudaStream_t st);
 void launch_to_float(int64_t n, const double* src, float* dst, cudaStream_t st);
+// after every level: each panel's L21 becomes Q = L21 L11^{-1} (what the solves read)
+void launch_panel_inverse(const DevPlan& p, double* val, const double* inv, cudaStream_t st);
 
 // ---- multi-RHS supernodal triangular solves (solve.cu) ----
 constexpr int kRhsTile = 64;     // right-hand sides per solve CTA; K is a multiple of this
@@ -60,7 +62,7 @@ constexpr int kSplitRows = 128;  // structure rows per backward split-K task
 template <typename T>
 struct SolveArgs {
     DevPlan p;
-    const T* val = nullptr;          // panels
+    const T* val = nullptr;          // panels: below the diagonal block, Q = L21 L11^{-1}
     const T* inv = nullptr;          // inverse diagonal blocks
     const T* R = nullptr;            // n x K right-hand sides (read only; unused with delta_src)
     T* B = nullptr;                  // n x K forward result, then solution (elimination order)

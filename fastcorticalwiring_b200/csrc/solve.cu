@@ -19,20 +19,23 @@
 // register tiles on the FMA pipes (a thread owns 4 rows x KT/16 columns in
 // 16-byte column groups).
 //
+// The panels below the diagonal blocks hold Q_s = L_rs inv(L_ss) (formed once
+// after the factorisation), so nothing waits for X_s:
+//
 // Forward (leaves -> root), multifrontal: supernode s forms
 //   W   = b_s - the children's update rows that land on s's columns
 //   X_s = inv(L_ss) W                                   (written to B)
-//   U_s = L_rs X_s + the children's update rows that land on s's structure
+//   U_s = Q_s W + the children's update rows that land on s's structure
 // and leaves U_s (nr x K) for its parent. Children's rows are listed per front
 // row in ascending child order and added in that order, so results are
-// deterministic. A supernode with a long structure is split into 64-row tasks
-// that each recompute X_s (cheap) and write their own rows of U_s.
+// deterministic. A supernode with a long structure is split into 64-row tasks;
+// each forms W and its own rows of U_s, and the first also X_s.
 //
-// Backward (root -> leaves): C = y_s - L_rs^T X_r (gather of the structure
-// rows, which belong to ancestors and are final; two chunks in flight),
-// X_s = inv(L_ss)^T C. Long structures are split over several CTAs (split-K);
-// each writes a partial sum, and the CTA that arrives last (atomic ticket, no
-// waiting) adds the partials in split order and finishes the supernode.
+// Backward (root -> leaves): X_s = inv(L_ss)^T y_s - Q_s^T X_r, where X_r are
+// the structure rows (ancestors, final; gathered two chunks in flight). Long
+// structures are split over several CTAs (split-K); each writes a partial sum
+// of Q_s^T X_r, and the CTA that arrives last (atomic ticket, no waiting) adds
+// the partials in split order and finishes the supernode.
 //
 // Heat right-hand sides are columns of the identity: the forward sweep builds
 // them from the source list, and only supernodes on a source's path to the
@@ -57,11 +60,16 @@ template <typename T>
 constexpr int wide_tile() { return sizeof(T) == 4 ? 128 : 64; }
 // Most children's update rows a forward CTA stages per gather chunk. The
 // launcher picks the count per level (SolveArgs::stage): none on levels without
-// children, else what keeps three FP32 CTAs (two FP64) on an SM.
+// children, else what keeps two CTAs on an SM (three for FP32 with KT = 64).
 template <typename T, int TR>
 constexpr int stage_rows() { return sizeof(T) == 4 ? 112 : 80; }
 template <typename T, int KT>
-constexpr int stage_used() { return sizeof(T) == 8 ? 80 : (KT == 128 ? 48 : 112); }
+constexpr int stage_used() { return sizeof(T) == 8 ? 80 : (KT == 128 ? 88 : 96); }
+// FP32 forward CTAs hold the inverse and the chunk's Q rows in two tiles (both
+// products start as soon as W is formed); FP64 tiles are twice the size, so
+// there the Q rows replace the inverse after X_s.
+template <typename T>
+constexpr bool separate_q() { return sizeof(T) == 4; }
 template <typename T>
 constexpr int vec() { return 16 / (int)sizeof(T); }  // elements per 16-byte vector
 
@@ -152,6 +160,12 @@ struct AccScalar {
 #pragma unroll
             for (int b = 0; b < NB; ++b) c[a][b] = T(0);
     }
+    __device__ __forceinline__ void negate() {
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+            for (int b = 0; b < NB; ++b) c[a][b] = -c[a][b];
+    }
 
     template <int MA>
     __device__ __forceinline__ void rows_n(const T* A, int lda, const T* Bm, int ldb, int depth) {
@@ -223,6 +237,13 @@ struct AccDmma {
     __device__ __forceinline__ void zero() {
 #pragma unroll
         for (int m = 0; m < MT; ++m) c[m][0] = c[m][1] = 0.0;
+    }
+    __device__ __forceinline__ void negate() {
+#pragma unroll
+        for (int m = 0; m < MT; ++m) {
+            c[m][0] = -c[m][0];
+            c[m][1] = -c[m][1];
+        }
     }
 
     static __device__ __forceinline__ void mma(double (&d)[2], double a, double b) {
@@ -406,10 +427,12 @@ template <typename T, int KT, int TR>
 __global__ void __launch_bounds__(NT, 3) k_fwd(SolveArgs<T> a, int32_t t0) {
     constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_fwd_a<T, TR>(), DP = depth_pad<T>();
     using AccT = Acc<T, KT, TR>;
+    constexpr bool kSepQ = separate_q<T>();
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* Wt = reinterpret_cast<T*>(smraw);   // TR x LW: W, then X, then this chunk's update rows
-    T* Lp = Wt + TR * LW;                   // TR x LA: inverse diagonal block, then the panel chunk
-    T* St = Lp + TR * LA;                   // a.stage x KT: children's update rows
+    T* Wt = reinterpret_cast<T*>(smraw);   // TR x LW: W, then this chunk's update rows
+    T* Li = Wt + TR * LW;                   // TR x LA: inverse diagonal block (first chunk)
+    T* Pn = kSepQ ? Li + TR * LA : Li;      // TR x LA: this chunk's rows of Q_s
+    T* St = Pn + TR * LA;                   // a.stage x KT: children's update rows
     __shared__ int grs[TR + 1];
     __shared__ unsigned char live[stage_rows<T, TR>()];
     const int2 task = a.tasks[t0 + blockIdx.x];
@@ -423,14 +446,25 @@ __global__ void __launch_bounds__(NT, 3) k_fwd(SolveArgs<T> a, int32_t t0) {
     const int64_t fb = p.sn_rowptr[s];
     const int q0 = chunk * TR;
     const int nq = nr > 0 ? min(TR, nr - q0) : 0;
+    const bool want_x = chunk == 0;
+    const bool q_early = nq > 0 && (kSepQ || !want_x);  // Q rows come with the first copies
+    const T* Q = a.val + p.sn_valptr[s] + (int64_t)(ns + q0) * ns;
 
-    // the inverse block, the right-hand side rows and the first children's rows
-    // are in flight together (identity right-hand sides are built in place)
-    const T* inv = a.inv + p.sn_invptr[s];
-    for (int e = tid; e < ns * ns; e += NT) {
-        const int i = e / ns, j = e - i * ns;
-        copy_async(&Lp[i * LA + j], inv + e);
+    // the inverse block, this chunk's rows of Q_s, the right-hand side rows and
+    // the first children's rows are in flight together (identity right-hand
+    // sides are built in place)
+    if (want_x) {
+        const T* inv = a.inv + p.sn_invptr[s];
+        for (int e = tid; e < ns * ns; e += NT) {
+            const int i = e / ns, j = e - i * ns;
+            copy_async(&Li[i * LA + j], inv + e);
+        }
     }
+    if (q_early)
+        for (int e = tid; e < nq * ns; e += NT) {
+            const int r = e / ns, j = e - r * ns;
+            copy_async(&Pn[r * LA + j], Q + e);
+        }
     if (a.delta_src) {
         for (int e = tid; e < ns * KT; e += NT) {
             const int f = e / KT, c = e - f * KT;
@@ -442,41 +476,46 @@ __global__ void __launch_bounds__(NT, 3) k_fwd(SolveArgs<T> a, int32_t t0) {
             copy16_async(Wt + f * LW + v * vec<T>(), a.R + (int64_t)(c0 + f) * K + k0 + v * vec<T>());
         }
     }
-    if (nsp > ns) {  // padded depth: zero in both operands (also for X below)
+    if (nsp > ns) {  // padded depth: zero in both operands
         zero_rows(Wt, LW, ns, nsp, KT);
-        zero_cols(Lp, LA, ns, ns, nsp);
+        if (want_x) zero_cols(Li, LA, ns, ns, nsp);
+        if (q_early) zero_cols(Pn, LA, nq, ns, nsp);
     }
     const GatherRange g1 = gather_open(a, fb, 0, ns, grs);
     if (g1.E > 0) gather_issue<T, KT, TR>(a, g1, 0, k0, St, live);
     copy_async_commit();
     gather_finish<T, KT, TR, true>(a, g1, k0, Wt, LW, ns, St, live, grs);
 
-    // X = inv(L_ss) W, written over W
-    AccT acc;
-    acc.zero();
-    acc.rows(Lp, LA, Wt, LW, nsp, ns);
-    __syncthreads();
-    acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(Wt + r * LW + c, v); });
-    __syncthreads();
-    if (chunk == 0) tile_rows_to_global<T, KT>(a.B + (int64_t)c0 * K + k0, K, Wt, LW, ns);
-    if (nq <= 0) return;
-
-    // U_s rows of this chunk = L_rs X + the children's rows landing on them; the
-    // panel rows take the inverse's place
-    const T* P = a.val + p.sn_valptr[s] + (int64_t)(ns + q0) * ns;
-    for (int e = tid; e < nq * ns; e += NT) {
-        const int r = e / ns, j = e - r * ns;
-        copy_async(&Lp[r * LA + j], P + e);
+    // the children's rows of this chunk's update rows arrive while X_s and U_s are formed
+    GatherRange g2{0, 0};
+    if (nq > 0) {
+        g2 = gather_open(a, fb, ns + q0, nq, grs);
+        if (g2.E > 0) gather_issue<T, KT, TR>(a, g2, 0, k0, St, live);
+        copy_async_commit();
     }
-    if (nsp > ns) zero_cols(Lp, LA, nq, ns, nsp);
-    const GatherRange g2 = gather_open(a, fb, ns + q0, nq, grs);
-    if (g2.E > 0) gather_issue<T, KT, TR>(a, g2, 0, k0, St, live);
-    copy_async_commit();
-    copy_async_wait();
-    __syncthreads();
+    AccT acc;
+    if (want_x) {  // X = inv(L_ss) W, straight from the registers to B
+        acc.zero();
+        acc.rows(Li, LA, Wt, LW, nsp, ns);
+        T* xb = a.B + (int64_t)c0 * K + k0;
+        acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(xb + (int64_t)r * K + c, v); });
+    }
+    if (nq <= 0) return;
+    if (!q_early) {  // one shared tile: the Q rows take the inverse's place now
+        __syncthreads();
+        for (int e = tid; e < nq * ns; e += NT) {
+            const int r = e / ns, j = e - r * ns;
+            copy_async(&Pn[r * LA + j], Q + e);
+        }
+        if (nsp > ns) zero_cols(Pn, LA, nq, ns, nsp);
+        copy_async_commit();
+        copy_async_wait();
+        __syncthreads();
+    }
+    // U_s rows of this chunk = Q_s W + the children's rows landing on them
     acc.zero();
-    acc.rows(Lp, LA, Wt, LW, nsp, nq);
-    __syncthreads();
+    acc.rows(Pn, LA, Wt, LW, nsp, nq);
+    __syncthreads();  // every thread is done reading W
     acc.visit(nq, [&](int r, int c, T* v) { st_n<T, AccT::V>(Wt + r * LW + c, v); });
     gather_finish<T, KT, TR, false>(a, g2, k0, Wt, LW, nq, St, live, grs);
     tile_rows_to_global<T, KT>(a.U + (a.uoff[s] + q0) * (int64_t)K + k0, K, Wt, LW, nq);
@@ -490,7 +529,7 @@ __global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
     using AccT = Acc<T, KT, TR>;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* buf = reinterpret_cast<T*>(smraw);
-    T* Cs = buf;             // TR x LW, after the gather
+    T* Ys = buf;             // TR x LW: y_s, after the gather
     T* Ms = buf + TR * LW;   // TR x LA inverse diagonal block, after the gather
     __shared__ int last_arrival;
     const int2 task = a.tasks[t0 + blockIdx.x];
@@ -566,30 +605,27 @@ __global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
         });
         if (tid == 0) a.counters[(int64_t)s * a.ktiles + blockIdx.y] = 0;
     }
-    // C = y - acc; X_s = inv(L_ss)^T C
-    const T* inv = a.inv + p.sn_invptr[s];
-    for (int e = tid; e < ns * ns; e += NT) {
-        const int i = e / ns, j = e - i * ns;
-        copy_async(&Ms[i * LA + j], inv + e);
+    // X_s = inv(L_ss)^T y_s - Q_s^T X_r (y_s = 0 off the sources' paths)
+    acc.negate();
+    if (!zero_y) {
+        const T* inv = a.inv + p.sn_invptr[s];
+        for (int e = tid; e < ns * ns; e += NT) {
+            const int i = e / ns, j = e - i * ns;
+            copy_async(&Ms[i * LA + j], inv + e);
+        }
+        for (int i = tid; i < ns * VPR; i += NT) {
+            const int r = i / VPR, v = i - r * VPR;
+            copy16_async(Ys + r * LW + v * vec<T>(), a.B + (int64_t)(c0 + r) * K + k0 + v * vec<T>());
+        }
+        copy_async_commit();
+        if (nsp > ns) {
+            zero_rows(Ms, LA, ns, nsp, TR);
+            zero_rows(Ys, LW, ns, nsp, KT);
+        }
+        copy_async_wait();
+        __syncthreads();
+        acc.cols(Ms, LA, Ys, LW, nsp, ns);
     }
-    copy_async_commit();
-    if (nsp > ns) {
-        zero_rows(Ms, LA, ns, nsp, TR);
-        zero_rows(Cs, LW, ns, nsp, KT);
-    }
-    acc.visit(ns, [&](int r, int c, T* v) {
-        T y[AccT::V];
-#pragma unroll
-        for (int q = 0; q < AccT::V; ++q) y[q] = T(0);
-        if (!zero_y) ld_n<T, AccT::V>(a.B + (int64_t)(c0 + r) * K + k0 + c, y);
-#pragma unroll
-        for (int q = 0; q < AccT::V; ++q) y[q] -= v[q];
-        st_n<T, AccT::V>(Cs + r * LW + c, y);
-    });
-    copy_async_wait();
-    __syncthreads();
-    acc.zero();
-    acc.cols(Ms, LA, Cs, LW, nsp, ns);
     T* out = a.B + (int64_t)c0 * K + k0;
     acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(out + (int64_t)r * K + c, v); });
 }
@@ -610,7 +646,8 @@ __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __res
 
 template <typename T, int KT, int TR>
 constexpr size_t fwd_smem(int stage = stage_rows<T, TR>()) {
-    return (size_t)(TR * ld_rows<T, KT>() + TR * ld_fwd_a<T, TR>() + stage * KT) * sizeof(T);
+    return (size_t)(TR * ld_rows<T, KT>() + (separate_q<T>() ? 2 : 1) * TR * ld_fwd_a<T, TR>() + stage * KT) *
+           sizeof(T);
 }
 template <typename T, int KT, int TR>
 constexpr size_t bwd_smem() {
