@@ -214,19 +214,48 @@ __device__ __forceinline__ double warp_sum(double v) {
 // with the other sources' work.
 constexpr int kMetricThreads = 256;
 
+// Each distance bin of the complete range is split into up to kSubBins sub-bins by
+// the same quotient hi / width that picks the bin, so that an evaluation at r can
+// take the faces below r's sub-bin as whole areas and skip the sub-bins above r
+// whose faces (and all later ones) lie beyond r.
+constexpr int kSubBins = 16;
+constexpr int kInfKey = 0x7f800000;  // lo_key(+inf)
+
+// Order-preserving int key of a float (for atomicMin) and back.
+__device__ __forceinline__ int lo_key(double lo) {
+    const int b = __float_as_int(__double2float_rd(lo));  // rounded down: a lower bound of lo
+    return b >= 0 ? b : b ^ 0x7fffffff;
+}
+__device__ __forceinline__ double key_lo(int k) { return (double)__int_as_float(k >= 0 ? k : k ^ 0x7fffffff); }
+
 struct SrcShared {
     union {
-        unsigned long long hist[kMaxBins + 1];  // face areas per bin, fixed point (order-free sums)
-        double pre[kMaxBins + 1];               // then the exclusive prefix sums of the bins' areas
+        unsigned long long hist[kMaxBins + 1];  // face areas per sub-bin, fixed point (order-free sums)
+        double pre[kMaxBins + 1];               // then the exclusive prefix sums of the sub-bins' areas
     };
-    int ptr[kMaxBins + 1];     // faces per bin -> exclusive prefix
-    int fill[kMaxBins];
+    int ptr[kMaxBins + 1];     // faces per sub-bin -> exclusive prefix -> (counting sort) inclusive prefix
     double red[16][4];
     double dred[16][5];
     double radii[kMaxTargets];
     double total, dglob;
+    int minlo[kMaxBins + 1];   // per sub-bin: a lower bound of its faces' lo (lo_key), then the suffix minima
     int nbins, rc, nlong, ntot, n_eval, bad, overflow;
+    int sb;                    // sub-bins per bin
 };
+
+// Sub-bins per bin for nbb complete bins: as many as the shared arrays hold.
+__device__ __forceinline__ int sub_bins(int nbb) {
+    int sb = kSubBins;
+    while (sb > 1 && nbb * sb > kMaxBins) sb >>= 1;
+    return sb;
+}
+
+// Sub-bin of quotient q = hi / width within its bin kb = bin_of(hi). (q - kb) * sb is
+// exact (Sterbenz, power-of-two scale), so sub-bin order follows q, and q follows hi.
+__device__ __forceinline__ int sub_of(double q, int kb, int sb) {
+    const int j = (int)((q - (double)kb) * sb);
+    return j < 0 ? 0 : (j >= sb ? sb - 1 : j);
+}
 
 // A source's distance field with its near-face bins (lean_geometry.py:117-299 restated over
 // the faces that can matter): bins [0, rc) are complete, larger bins are never queried.
@@ -243,7 +272,7 @@ struct Field {
         const int k = (int)(dmax / a->width);
         return k < 0 ? 0 : k;
     }
-    __device__ double prefix_at(int k) const { return k <= s->rc && k < s->nbins ? s->pre[k] : s->total; }
+    __device__ double prefix_at(int k) const { return k <= s->rc && k < s->nbins ? s->pre[k * s->sb] : s->total; }
 
     __device__ void face_term(int f, double r, int mode, double& x1, double& x2) const {
         const int* fv = a->fv;
@@ -271,15 +300,28 @@ struct Field {
         }
     }
 
-    // Faces with bin in [kr, kend) plus long faces with bin >= kend, summed by one warp.
-    __device__ void band_sum(int kr, int kend, double r, int mode, double& s1, double& s2) const {
+    // Faces with bin in [kr, kend) plus long faces with bin >= kend, summed by one warp;
+    // `inside` + s1 is the area (mode 0). Within complete bins only the sub-bins
+    // [j0, j1) are visited: every face of a lower sub-bin has hi < r (face_cdf would
+    // return its whole area, summed into `inside` from the prefix), and every face
+    // from sub-bin j1 on has lo >= r (both of its terms are exactly zero).
+    __device__ void band_sum(int kr, int kend, double r, int mode, double& s1, double& s2, double& inside) const {
         const int lane = threadIdx.x & 31;
         double x1 = 0.0, x2 = 0.0;
         const int* fv = a->fv;
         if (kend <= s->rc) {
+            const int sb = s->sb;
+            const int j0 = kr * sb + sub_of(r / a->width, kr, sb);
+            const int jend = kend * sb;  // at most j0 + 2 * kSubBins
+            // j1: the first sub-bin above j0 from which on every binned face has lo >= r
+            const int jc = j0 + 1 + lane;
+            const unsigned far = __ballot_sync(0xffffffffu, jc < jend && key_lo(s->minlo[jc]) >= r);
+            const int j1 = far ? j0 + __ffs(far) : jend;
+            inside = s->pre[j0];
+            // sub-bin j's faces are band[ptr[j-1], ptr[j]) after the counting sort
+            int j = (j0 > 0 ? s->ptr[j0 - 1] : 0) + lane;
+            const int je = s->ptr[j1 - 1];
             // four records per lane in flight
-            int j = s->ptr[kr] + lane;
-            const int je = s->ptr[kend];
             for (; j + 96 < je; j += 128) {
                 int4 q[4];
                 double dd[4][3];
@@ -299,6 +341,7 @@ struct Field {
                 rec_term(q0, dv(q0.y), dv(q0.z), dv(q0.w), r, mode, x1, x2);
             }
         } else {  // beyond the complete bins: scan every face (not reached for healthy fields)
+            inside = prefix_at(kr);
             for (int f = lane; f < a->nf; f += 32) {
                 const double d0 = dv(fv[3 * f]), d1 = dv(fv[3 * f + 1]), d2 = dv(fv[3 * f + 2]);
                 if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
@@ -321,9 +364,9 @@ struct Field {
         const int kr = (int)(r / a->width);
         if (kr >= s->nbins) { A = s->total; dA = 0.0; return; }
         const int kend = min(kr + 2, s->nbins);
-        double b1, b2;
-        band_sum(kr, kend, r, 0, b1, b2);
-        A = prefix_at(kr) + b1;
+        double b1, b2, inside;
+        band_sum(kr, kend, r, 0, b1, b2, inside);
+        A = inside + b1;
         dA = b2;
     }
 
@@ -333,8 +376,8 @@ struct Field {
         const int kr = (int)(r / a->width);
         if (kr >= s->nbins) return 0.0;
         const int kend = min(kr + 2, s->nbins);
-        double b1, b2;
-        band_sum(kr, kend, r, 1, b1, b2);
+        double b1, b2, inside;
+        band_sum(kr, kend, r, 1, b1, b2, inside);
         return b1;
     }
 
@@ -484,12 +527,15 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
     Field<T> F{d, &a, &S, band, longf};
     for (int attempt = 0; attempt < 32; ++attempt) {
         const int rc = S.rc;
-        for (int i = tid; i <= kMaxBins; i += bs) {
+        const int nbb = min(rc + 1, nbins);  // complete bins [0, nbb)
+        const int sb = sub_bins(nbb);
+        const int nsub = nbb * sb;
+        for (int i = tid; i <= nsub; i += bs) {
             S.hist[i] = 0ull;
             S.ptr[i] = 0;
-            if (i < kMaxBins) S.fill[i] = 0;
+            S.minlo[i] = kInfKey;
         }
-        if (tid == 0) { S.nlong = 0; S.overflow = 0; }
+        if (tid == 0) { S.nlong = 0; S.overflow = 0; S.sb = sb; }
         __syncthreads();
         const double R = rc >= nbins ? INFINITY : rc * w;
         // vertices closer than R: the shift kernel's near list when R is its radius
@@ -538,57 +584,76 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
                         if (d1 > hi) hi = d1;
                         if (d2 < lo) lo = d2;
                         if (d2 > hi) hi = d2;
-                        const int kb = F.bin_of(hi);
+                        const double q = hi / w;  // F.bin_of's quotient
+                        const int kb = q < 1.0 ? 0 : (int)q;
+                        const int jb = kb * sb + sub_of(q, kb, sb);
                         if (pass == 0) {
                             if (hi - lo > w) longf[atomicAdd(&S.nlong, 1)] = f;
-                            if (kb <= rc && kb < kMaxBins) {
-                                atomicAdd(&S.hist[kb], (unsigned long long)fx[u]);
-                                atomicAdd(&S.ptr[kb], 1);
+                            if (kb < nbb) {
+                                atomicAdd(&S.hist[jb], (unsigned long long)fx[u]);
+                                atomicAdd(&S.ptr[jb], 1);
+                                atomicMin(&S.minlo[jb], lo_key(lo));
                             }
-                        } else if (kb <= rc && kb < kMaxBins) {
-                            band[S.ptr[kb] + atomicAdd(&S.fill[kb], 1)] = rec[u];
+                        } else if (kb < nbb) {
+                            band[atomicAdd(&S.ptr[jb], 1)] = rec[u];  // ptr[jb] ends at the next sub-bin's start
                         }
                     }
                 }
             }
             __syncthreads();
             if (pass == 0) {
-                // exclusive prefix sums over bins [0, min(rc, nbins-1)] by warp 0
+                // exclusive prefix sums over the sub-bins [0, nsub) by warp 0, exact in
+                // fixed point, each rounded once to an area
                 if (warp == 0) {
-                    const int nbb = min(rc + 1, nbins);
-                    const int chunk = (nbb + 31) / 32;
-                    const int b0 = min(lane * chunk, nbb), b1 = min(b0 + chunk, nbb);
-                    double sa = 0.0;
+                    const int chunk = (nsub + 31) / 32;
+                    const int b0 = min(lane * chunk, nsub), b1 = min(b0 + chunk, nsub);
+                    unsigned long long sa = 0ull;
                     int sc = 0;
-                    for (int b = b0; b < b1; ++b) { sa += (double)S.hist[b] * a.area_unscale; sc += S.ptr[b]; }
-                    double ea = sa;
+                    for (int b = b0; b < b1; ++b) { sa += S.hist[b]; sc += S.ptr[b]; }
+                    unsigned long long ea = sa;
                     int ec = sc;
                     for (int off = 1; off < 32; off <<= 1) {
-                        const double ta = __shfl_up_sync(0xffffffffu, ea, off);
+                        const unsigned long long ta = __shfl_up_sync(0xffffffffu, ea, off);
                         const int tc = __shfl_up_sync(0xffffffffu, ec, off);
                         if (lane >= off) { ea += ta; ec += tc; }
                     }
-                    double ra = ea - sa;
+                    unsigned long long ra = ea - sa;
                     int rcn = ec - sc;
                     for (int b = b0; b < b1; ++b) {
-                        const double xa = (double)S.hist[b] * a.area_unscale;
+                        const unsigned long long xa = S.hist[b];
                         const int xc = S.ptr[b];
-                        S.pre[b] = ra;
+                        S.pre[b] = (double)ra * a.area_unscale;
                         S.ptr[b] = rcn;
                         ra += xa;
                         rcn += xc;
                     }
                     if (lane == 31) {
                         S.ntot = ec;
-                        S.pre[nbb] = ea;
-                        S.ptr[nbb] = ec;
+                        S.pre[nsub] = (double)ea * a.area_unscale;
+                        S.ptr[nsub] = ec;
+                    }
+                } else if (warp == 1) {
+                    // suffix minima of the sub-bins' lower bounds of lo
+                    const int chunk = (nsub + 31) / 32;
+                    const int b0 = min(lane * chunk, nsub), b1 = min(b0 + chunk, nsub);
+                    int mk = kInfKey;
+                    for (int b = b0; b < b1; ++b) mk = min(mk, S.minlo[b]);
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const int t = __shfl_down_sync(0xffffffffu, mk, off);
+                        if (lane + off < 32) mk = min(mk, t);
+                    }
+                    int after = __shfl_down_sync(0xffffffffu, mk, 1);
+                    if (lane == 31) after = kInfKey;
+                    for (int b = b1 - 1; b >= b0; --b) {
+                        after = min(after, S.minlo[b]);
+                        S.minlo[b] = after;
                     }
                 }
                 __syncthreads();
             }
         }
         // enough? the largest target must be enclosed two bins below the cut
-        bool ok = rc >= nbins || (rc >= 2 && S.pre[rc - 2] >= tmax);
+        bool ok = rc >= nbins || (rc >= 2 && S.pre[(rc - 2) * sb] >= tmax);
         if (ok) break;
         __syncthreads();
         if (tid == 0) S.rc = min(nbins, 2 * rc + 4);
