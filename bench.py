@@ -553,7 +553,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=4096, help="sources per step")
     ap.add_argument("--block-k", type=int, default=1024)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
-    ap.add_argument("--pipeline-depth", type=int, default=3, help="blocks in flight on separate streams")
+    ap.add_argument("--pipeline-depth", type=int, default=4, help="blocks in flight on separate streams")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--leaf-size", type=int, default=64, help="nested-dissection leaf size")
     ap.add_argument("--relax", type=int, default=64, help="relaxed supernode amalgamation (columns)")

@@ -19,7 +19,7 @@ from . import engine as E
 from . import mesh as M
 
 DEFAULT_K = (64, 128, 256, 512, 1024)
-DEFAULT_DEPTH = (1, 2, 3)
+DEFAULT_DEPTH = (1, 2, 3, 4)
 
 
 def autotune(pm: M.PreparedMesh, scales=M.RUNNER_SCALES, n_between=3, precision="mixed", ks=DEFAULT_K,

@@ -265,7 +265,7 @@ int validate_params(const fcw_params* p) {
     if (p->leaf_size < 1 || p->max_width < 1 || p->max_width > fcw::kMaxWidth)
         return fail(FCW_E_INVALID, "max_width must be in [1, 64] and leaf_size >= 1");
     if (p->relax < 1 || p->relax > p->max_width) return fail(FCW_E_INVALID, "relax must be in [1, max_width]");
-    if (p->pipeline_depth < 1 || p->pipeline_depth > 4) return fail(FCW_E_INVALID, "pipeline_depth must be in [1, 4]");
+    if (p->pipeline_depth < 1 || p->pipeline_depth > 8) return fail(FCW_E_INVALID, "pipeline_depth must be in [1, 8]");
     return FCW_OK;
 }
 
@@ -775,13 +775,17 @@ int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, do
     a.near_list = e->cw().near_list;
     a.near_count = e->cw().near_count;
     {
-        // near radius: a flat disc holding twice the largest reachable target, in whole bins
+        // near radius: a flat disc holding twice the largest reachable target, in whole bins.
+        // A source first tries the cut of a flat disc holding the target itself plus four
+        // bins (enough for most fields: the radius is two bins below the cut), then the
+        // near radius, both from the near list.
         double tmax = 0.0;
         for (int32_t i = 0; i < nt; ++i)
             if (targets[i] > tmax && targets[i] <= e->lean_total) tmax = targets[i];
-        const double r0 = std::sqrt(2.0 * tmax / 3.141592653589793);
-        a.near_bins = (int32_t)std::ceil(r0 / e->mesh.bin_width) + 2;
+        const double pi = 3.141592653589793;
+        a.near_bins = (int32_t)std::ceil(std::sqrt(2.0 * tmax / pi) / e->mesh.bin_width) + 2;
         a.near_radius = (double)a.near_bins * e->mesh.bin_width;
+        a.first_bins = std::min(a.near_bins, (int32_t)std::ceil(std::sqrt(tmax / pi) / e->mesh.bin_width) + 4);
     }
     a.src = e->cw().src;
     a.band = e->cw().band;
@@ -839,7 +843,7 @@ void fcw_default_params(fcw_params* p) {
     p->relax = 64;
     p->build_mixed = 1;
     p->device = 0;
-    p->pipeline_depth = 3;
+    p->pipeline_depth = 4;
 }
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between) {

@@ -155,6 +155,7 @@ struct MetricArgs {
     double* partials = nullptr;         // ntiles x K x 8 partial statistics
     double near_radius = 0.0;           // = near_bins * width
     int32_t near_bins = 0;
+    int32_t first_bins = 0;             // cut of a source's first attempt (<= near_bins)
     int32_t* near_list = nullptr;       // K x n: vertices closer than near_radius, per source
     int32_t* near_count = nullptr;      // K
 };

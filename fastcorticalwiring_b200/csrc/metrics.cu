@@ -241,6 +241,7 @@ struct SrcShared {
     int minlo[kMaxBins + 1];   // per sub-bin: a lower bound of its faces' lo (lo_key), then the suffix minima
     int nbins, rc, nlong, ntot, n_eval, bad, overflow;
     int sb;                    // sub-bins per bin
+    int nstage;                // binned faces staged (unsorted) at the top of the band array
 };
 
 // Sub-bins per bin for nbb complete bins: as many as the shared arrays hold.
@@ -430,12 +431,13 @@ struct Field {
 // Everything computed from one source's field, one CTA per source:
 //   1. the health screen, MSD and global max from the shift kernel's partial sums,
 //      and the distance to boundary;
-//   2. the faces that have a corner closer than rc*w (rc starts at the near radius
-//      of the shift kernel's near lists), each emitted once by its first near corner
-//      through the vertex->face incidence lists: their area histogram, counting sort
-//      by bin and the long-face list (lean_geometry.py:117-180 on these faces). Bins
-//      below rc are complete. If the largest target is not enclosed two bins below rc,
-//      rc grows (up to every bin, scanning all vertices) and step 2 repeats;
+//   2. the faces that have a corner closer than rc*w (rc starts at a first cut inside
+//      the radius of the shift kernel's near lists), each emitted once by its first
+//      near corner through the vertex->face incidence lists: their area histogram,
+//      counting sort by sub-bin and the long-face list (lean_geometry.py:117-180 on
+//      these faces). Bins below rc are complete. If the largest target is not enclosed
+//      two bins below rc, rc grows (to the near lists' radius, then up to every bin,
+//      scanning all vertices) and step 2 repeats;
 //   3. one warp per target: bracket + safeguarded Newton + perimeter; then the samples.
 template <typename T>
 __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
@@ -508,7 +510,7 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
         S.nbins = nb < (double)(kMaxBins - 2) ? (int)nb + 2 : kMaxBins + 1;
         S.total = a.total_area;
         S.n_eval = 0;
-        S.rc = a.near_bins;
+        S.rc = a.first_bins;
     }
     __syncthreads();
     // A flagged field gets no geometry (core_analysis.py:1558-1564).
@@ -535,14 +537,32 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
             S.ptr[i] = 0;
             S.minlo[i] = kInfKey;
         }
-        if (tid == 0) { S.nlong = 0; S.overflow = 0; S.sb = sb; }
+        if (tid == 0) { S.nlong = 0; S.overflow = 0; S.sb = sb; S.nstage = 0; }
         __syncthreads();
         const double R = rc >= nbins ? INFINITY : rc * w;
-        // vertices closer than R: the shift kernel's near list when R is its radius
-        const bool listed = rc == a.near_bins && rc < nbins;
+        // vertices closer than R: from the shift kernel's near list while R is within its radius
+        const bool listed = rc <= a.near_bins && rc < nbins;
         const int nv_scan = listed ? a.near_count[k] : a.n;
         const int32_t* nl = a.near_list + (int64_t)k * a.n;
         for (int pass = 0; pass < 2; ++pass) {  // 0: histogram + long faces, 1: counting sort
+            // pass 0 also stages each binned face at the top of the band array; while the
+            // staged list and the sorted one (both ntot long) cannot overlap, pass 1 sorts
+            // the staged list instead of walking the incidences again
+            if (pass == 1 && 2 * S.ntot <= a.nf) {
+                const int ntot = S.ntot;
+                for (int p = tid; p < ntot; p += bs) {
+                    const int4 rq = band[a.nf - 1 - p];
+                    const double d0 = (double)d[rq.y], d1 = (double)d[rq.z], d2 = (double)d[rq.w];
+                    double hi = d0;  // as in pass 0
+                    if (d1 > hi) hi = d1;
+                    if (d2 > hi) hi = d2;
+                    const double q = hi / w;
+                    const int kb = q < 1.0 ? 0 : (int)q;
+                    band[atomicAdd(&S.ptr[kb * sb + sub_of(q, kb, sb)], 1)] = rq;
+                }
+                __syncthreads();
+                continue;
+            }
             for (int ii = tid; ii < nv_scan; ii += bs) {
                 const int i = listed ? nl[ii] : ii;
                 const double di = (double)d[i];
@@ -593,6 +613,7 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
                                 atomicAdd(&S.hist[jb], (unsigned long long)fx[u]);
                                 atomicAdd(&S.ptr[jb], 1);
                                 atomicMin(&S.minlo[jb], lo_key(lo));
+                                band[a.nf - 1 - atomicAdd(&S.nstage, 1)] = rec[u];
                             }
                         } else if (kb < nbb) {
                             band[atomicAdd(&S.ptr[jb], 1)] = rec[u];  // ptr[jb] ends at the next sub-bin's start
@@ -656,7 +677,7 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
         bool ok = rc >= nbins || (rc >= 2 && S.pre[(rc - 2) * sb] >= tmax);
         if (ok) break;
         __syncthreads();
-        if (tid == 0) S.rc = min(nbins, 2 * rc + 4);
+        if (tid == 0) S.rc = rc < a.near_bins ? a.near_bins : min(nbins, 2 * rc + 4);
         __syncthreads();
     }
     if (S.rc >= nbins) {

@@ -48,7 +48,7 @@ typedef struct fcw_params {
     int32_t relax;              /* etree subtrees of at most this many columns become one supernode */
     int32_t build_mixed;        /* also factor the grounded FP32 Poisson operator */
     int32_t device;             /* CUDA device ordinal */
-    int32_t pipeline_depth;     /* blocks in flight on separate streams in the device metrics path (1-4) */
+    int32_t pipeline_depth;     /* blocks in flight on separate streams in the device metrics path (1-8) */
 } fcw_params;
 
 typedef struct fcw_info {
@@ -92,7 +92,7 @@ enum {
     FCW_N_STAGES = 7
 };
 
-/* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 64, mixed on, 3 blocks in flight). */
+/* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 64, mixed on, 4 blocks in flight). */
 void fcw_default_params(fcw_params* p);
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between);
