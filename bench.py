@@ -287,6 +287,7 @@ def run_gpu(args):
     t0 = time.perf_counter()
     eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k, pipeline_depth=args.pipeline_depth,
                        leaf_size=args.leaf_size, relax=args.relax)
+    eng.graphs(not args.no_graphs)
     build_s = time.perf_counter() - t0
     info = eng.info()
 
@@ -408,7 +409,7 @@ def run_gpu(args):
             "engine": {"factor_ms": info["factor_ms"], "analyze_ms": info["analyze_ms"], "build_s": build_s,
                        "n_supernodes": info["n_supernodes"], "n_levels": info["n_levels"],
                        "nnz_factor": info["nnz_factor"], "device_bytes": info["device_bytes"],
-                       "pipeline_depth_held": info["pipeline_depth"]},
+                       "pipeline_depth_held": info["pipeline_depth"], "cuda_graphs": not args.no_graphs},
         }
         line.update(extra)
         if tuned is not None:
@@ -562,6 +563,7 @@ def main(argv=None):
     ap.add_argument("--fp64-sample", type=int, default=16)
     ap.add_argument("--ref-sources-per-core", type=int, default=2)
     ap.add_argument("--quick", action="store_true", help="skip the FP64 forms and the accuracy check")
+    ap.add_argument("--no-graphs", action="store_true", help="launch each block's kernels directly")
     ap.add_argument("--autotune", action="store_true", help="choose block size and depth on the mesh first")
     ap.add_argument("--serving", action="store_true", help="run the serving stream instead (own JSON line)")
     ap.add_argument("--serving-jobs", type=int, default=64)

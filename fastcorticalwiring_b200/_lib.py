@@ -25,7 +25,7 @@ EXPORTED = (
     "fcw_engine_create", "fcw_engine_info", "fcw_engine_destroy", "fcw_compute_distance",
     "fcw_compute_distances", "fcw_compute_metrics", "fcw_compute_metrics_device", "fcw_synchronize",
     "fcw_heat_solve_device", "fcw_divergence_device", "fcw_poisson_solve_device", "fcw_field_metrics_device",
-    "fcw_engine_profile", "fcw_engine_stage_times", "fcw_field_metrics_static",
+    "fcw_engine_profile", "fcw_engine_graphs", "fcw_engine_stage_times", "fcw_field_metrics_static",
     "fcw_samples_capacity", "fcw_assemble_samples_device", "fcw_assemble_samples",
 )
 STAGES = ("heat_fwd", "heat_bwd", "divergence", "poisson_fwd", "poisson_bwd", "shift", "metrics")
@@ -98,6 +98,7 @@ def load():
         "fcw_compute_metrics_device": (ctypes.c_int, [P, P, I64, I32, P, I32, I32, D, P, P]),
         "fcw_synchronize": (ctypes.c_int, [P, P]),
         "fcw_engine_profile": (ctypes.c_int, [P, ctypes.c_int]),
+        "fcw_engine_graphs": (ctypes.c_int, [P, ctypes.c_int]),
         "fcw_engine_stage_times": (ctypes.c_int, [P, P, I32, P]),
         "fcw_heat_solve_device": (ctypes.c_int, [P, P, I32, P, P]),
         "fcw_divergence_device": (ctypes.c_int, [P, P, I32, P, P]),

@@ -58,6 +58,27 @@ __global__ void k_map_sources(int64_t n, const int32_t* __restrict__ sources, co
     out[k] = v;
 }
 
+// The block's inputs into its workspace descriptor (ahead of the block's launch chain).
+__global__ void k_set_block(fcw::BlockDesc* d, const int32_t* sources, int64_t n, double* out) {
+    d->sources = sources;
+    d->n = n;
+    d->out = out;
+}
+
+// k_map_sources with the block's sources from the descriptor.
+__global__ void k_map_block_sources(const fcw::BlockDesc* __restrict__ d, const int32_t* __restrict__ iperm,
+                                    int32_t nv, int32_t K, int32_t* __restrict__ out, int* __restrict__ err) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K) return;
+    int v = -1;
+    if (k < d->n) {
+        const int s = d->sources[k];
+        if (s >= 0 && s < nv) v = iperm[s];
+        else atomicOr(err, fcw::KERR_ARGS);
+    }
+    out[k] = v;
+}
+
 // d (k rows, caller vertex order) -> Y (n x K vertex-major, elimination order); columns >= k are zero.
 __global__ void k_fields_in(int32_t n, int32_t k, int32_t K, const double* __restrict__ d,
                             const int32_t* __restrict__ iperm, double* __restrict__ Y) {
@@ -93,6 +114,19 @@ struct Workspace {
     std::vector<std::pair<int, cudaEvent_t>> marks;  // stage timeline on this workspace
     double* part = nullptr;     // backward split-K partial sums
     int* counters = nullptr;    // split-K arrival tickets, zero at rest
+    fcw::BlockDesc* desc = nullptr;     // the current block's inputs (device)
+    // the block's launch chain captured as CUDA graphs, one per set of arguments (a few)
+    struct Graph {
+        std::vector<double> key;
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;           // kernels in the graph
+    };
+    std::vector<Graph> graphs;
+    void drop_graph() {
+        for (auto& g : graphs)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
 };
 
 struct fcw_engine {
@@ -143,6 +177,7 @@ struct fcw_engine {
     double lean_total = 0.0;  // sum of the lean face areas (the prefix total of a finite field)
     // stage timeline (CUDA events on the working stream), off unless enabled
     bool prof_on = false;
+    bool graphs_on = true;  // replay each workspace's captured launch chain
     std::vector<cudaEvent_t> event_pool;
     double stage_ms[FCW_N_STAGES] = {0};
     int64_t launches = 0;
@@ -194,6 +229,7 @@ struct fcw_engine {
         for (auto& a : allocs) cudaFreeAsync(a.first, stream);
         if (stream) cudaStreamSynchronize(stream);
         for (auto& w : pool) {
+            w.drop_graph();
             for (auto& m : w.marks) cudaEventDestroy(m.second);
             if (w.done) cudaEventDestroy(w.done);
             if (w.stream) cudaStreamDestroy(w.stream);
@@ -590,9 +626,10 @@ int ensure_one(fcw_engine* e, Workspace& w, int32_t K, int32_t stride) {
     const int32_t Kn = std::max(K, w.K);
     const int32_t sn = std::max(stride, w.out_stride);
     void* old[] = {w.Bh, w.Bp64, w.Y, w.dT64, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
-                   w.counters, w.partials, w.near_list, w.near_count};
+                   w.counters, w.partials, w.near_list, w.near_count, w.desc};
     for (void* p : old)
         if (p) e->release(p);
+    w.drop_graph();  // its launches name the old buffers
     cudaStream_t stream = w.stream;
     cudaEvent_t done = w.done;
     w = Workspace{};
@@ -619,6 +656,7 @@ int ensure_one(fcw_engine* e, Workspace& w, int32_t K, int32_t stride) {
     const int64_t nctr = (int64_t)std::max<int32_t>(e->sym.nsuper, 1) * (Kn / fcw::kRhsTile);
     FCW_TRY(e->dalloc(&w.counters, (size_t)nctr));
     FCW_CUDA(cudaMemset(w.counters, 0, nctr * sizeof(int)));
+    FCW_TRY(e->dalloc(&w.desc, 1));
     w.K = Kn;
     w.out_stride = sn;
     return FCW_OK;
@@ -636,9 +674,10 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
         for (size_t j = i; j < e->pool.size(); ++j) {
             Workspace& w = e->pool[j];
             void* bufs[] = {w.Bh, w.Bp64, w.Y, w.dT64, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
-                            w.counters, w.partials, w.near_list, w.near_count};
+                            w.counters, w.partials, w.near_list, w.near_count, w.desc};
             for (void* p : bufs)
                 if (p) e->release(p);
+            w.drop_graph();
             for (auto& m : w.marks) cudaEventDestroy(m.second);
             if (w.done) cudaEventDestroy(w.done);
             if (w.stream) cudaStreamDestroy(w.stream);
@@ -1015,6 +1054,64 @@ int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host) {
     return fcw_compute_distances(e, &source, 1, FCW_PREC_FP64, out_host);
 }
 
+namespace {
+
+// One block's launch chain on workspace w, its inputs in w.desc: source mapping,
+// distances, metrics. With graphs on (and the stage timeline off) the chain is
+// captured once per workspace and set of arguments, and replayed for later blocks.
+int block_chain(fcw_engine* e, Workspace& w, int32_t K, int32_t precision, fcw::MetricArgs& a,
+                const double* targets, int32_t nt, int32_t nb, double eps) {
+    auto launch = [&]() {
+        k_map_block_sources<<<(K + 127) / 128, 128, 0, w.stream>>>(w.desc, e->iperm_d, (int32_t)e->sym.n, K, w.src,
+                                                                   e->err_d);
+        e->launches += 1;
+        distances_block(e, K, precision, w.stream, &a);
+        if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, w.dT32, w.stream);
+        else metrics_block<double>(e, a, w.dT64, w.stream);
+    };
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    FCW_CUDA(cudaStreamIsCapturing(w.stream, &cs));
+    if (!e->graphs_on || e->prof_on || cs != cudaStreamCaptureStatusNone) {  // (inside a caller's capture: join it)
+        launch();
+        return FCW_OK;
+    }
+    std::vector<double> key = {(double)K, (double)precision, (double)nt, (double)nb, eps};
+    key.insert(key.end(), targets, targets + nt);
+    Workspace::Graph* hit = nullptr;
+    for (auto& g : w.graphs)
+        if (g.key == key) hit = &g;
+    if (!hit) {
+        constexpr size_t kMaxGraphs = 4;  // e.g. a full block and a call's last, partial one
+        if (w.graphs.size() >= kMaxGraphs) {
+            cudaGraphExecDestroy(w.graphs.front().exec);
+            w.graphs.erase(w.graphs.begin());
+        }
+        const int64_t l0 = e->launches;
+        FCW_CUDA(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal));
+        launch();
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(w.stream, &g);
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        const int64_t captured = e->launches - l0;  // kernels in the chain (counted when it runs)
+        e->launches = l0;
+        if (ce != cudaSuccess) {  // not capturable here: launch directly from now on
+            cudaGetLastError();
+            e->graphs_on = false;
+            launch();
+            return FCW_OK;
+        }
+        w.graphs.push_back({key, exec, captured});
+        hit = &w.graphs.back();
+    }
+    FCW_CUDA(cudaGraphLaunch(hit->exec, w.stream));
+    e->launches += hit->launches;
+    return FCW_OK;
+}
+
+}  // namespace
+
 int fcw_compute_metrics_device(fcw_engine* e, const int32_t* sources_dev, int64_t n, int32_t precision,
                                const double* targets, int32_t nt, int32_t nb, double eps, double* out_dev,
                                void* stream) {
@@ -1045,13 +1142,10 @@ int fcw_compute_metrics_device(fcw_engine* e, const int32_t* sources_dev, int64_
         fcw::MetricArgs a;
         rc = metric_args(e, targets, nt, nb, eps, K, a);
         if (rc != FCW_OK) break;
-        a.out = out_dev + b0 * stride;
-        k_map_sources<<<(K + 127) / 128, 128, 0, w.stream>>>(nbk, sources_dev + b0, e->iperm_d, (int32_t)e->sym.n, K,
-                                                             w.src, e->err_d);
+        a.desc = w.desc;
+        k_set_block<<<1, 1, 0, w.stream>>>(w.desc, sources_dev + b0, nbk, out_dev + b0 * stride);
         e->launches += 1;
-        distances_block(e, K, precision, w.stream, &a);
-        if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, w.dT32, w.stream);
-        else metrics_block<double>(e, a, w.dT64, w.stream);
+        rc = block_chain(e, w, K, precision, a, targets, nt, nb, eps);
     }
     for (size_t i = 0; i < used; ++i) {
         FCW_CUDA(cudaEventRecord(e->pool[i].done, e->pool[i].stream));
@@ -1173,6 +1267,12 @@ int fcw_assemble_samples(fcw_engine* e, const double* records, int64_t n, int32_
     FCW_CUDA(cudaMemcpyAsync(areas, e->hsa_d, n * cap * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
     FCW_CUDA(cudaMemcpyAsync(count, e->hcnt_d, n * sizeof(int32_t), cudaMemcpyDeviceToHost, e->stream));
     FCW_CUDA(cudaStreamSynchronize(e->stream));
+    return FCW_OK;
+}
+
+int fcw_engine_graphs(fcw_engine* e, int enable) {
+    FCW_TRY(check_engine(e));
+    e->graphs_on = enable != 0;
     return FCW_OK;
 }
 

@@ -123,6 +123,14 @@ void launch_shift_transpose(int32_t n, int32_t K, const Tin* phi, const int32_t*
 void launch_permute_rows(int32_t n, int32_t cols, const double* in, int32_t in_ld, const int32_t* in_idx,
                          double* out, int32_t out_ld, const int32_t* out_idx, cudaStream_t st);
 
+// A block's inputs in the pipelined metrics path, read on the device, so that the
+// launch chain captured once per workspace serves every block.
+struct BlockDesc {
+    const int32_t* sources = nullptr;  // the block's sources (caller's order)
+    int64_t n = 0;                     // sources in the block (<= K)
+    double* out = nullptr;             // the block's records (n * stride)
+};
+
 struct MetricArgs {
     int32_t n = 0, nf = 0, nsrc = 0, stride = 0, n_targets = 0, n_between = 0, n_boundary = 0;
     const double* coords = nullptr;     // n*3, elimination order
@@ -148,6 +156,7 @@ struct MetricArgs {
     int4* band = nullptr;               // nsrc * nf scratch: near faces (face, corners) sorted by bin
     int32_t* longf = nullptr;           // nsrc * nf scratch: near long faces
     double* out = nullptr;              // nsrc * stride
+    const BlockDesc* desc = nullptr;    // when set, the records go to desc->out instead
     int* err = nullptr;
     // shift + statistics (k_shift_stats) -> per-source kernel
     int32_t K = 0;                      // columns of the block (partials' leading dimension)

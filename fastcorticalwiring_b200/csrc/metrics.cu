@@ -449,7 +449,7 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
     const int lane = tid & 31, warp = tid >> 5, nwarps = bs >> 5;
     const int nt = a.n_targets, m = a.n_between;
     const int ne = nt > 0 ? (nt - 1) * m : 0;
-    double* o = a.out + (int64_t)k * a.stride;
+    double* o = (a.desc ? a.desc->out : a.out) + (int64_t)k * a.stride;
     const double nan = __longlong_as_double(0x7ff8000000000000LL);
     const T* d = dT + (int64_t)k * a.n;
     int4* band = a.band + (int64_t)k * a.nf;

@@ -123,6 +123,10 @@ class HeatEngine:
                                                     c, _lib.ptr(radii), _lib.ptr(areas), _lib.ptr(counts)))
         return radii, areas, counts
 
+    def graphs(self, enable=True) -> None:
+        """Replay each workspace's captured launch chain (the default) or launch blocks directly."""
+        _lib.check(_lib.load().fcw_engine_graphs(self.handle, int(bool(enable))))
+
     def profile(self, enable=True) -> None:
         """Turn the per-stage CUDA-event timeline on/off (and reset it)."""
         _lib.check(_lib.load().fcw_engine_profile(self.handle, int(bool(enable))))

@@ -167,6 +167,13 @@ int fcw_assemble_samples_device(const double* records_dev, int64_t n, int32_t n_
 int fcw_assemble_samples(fcw_engine* e, const double* records, int64_t n, int32_t n_targets, int32_t n_between,
                          const double* targets, double boundary_cap, float* radii, float* areas, int32_t* count);
 
+/* CUDA graphs in fcw_compute_metrics(_device): enable (1, the default) / disable (0).
+ * Each workspace captures its block's launch chain once per set of arguments (K,
+ * precision, targets, n_between, eps) and replays it for later blocks; the block's
+ * sources and output pointer reach the chain through a device descriptor. While the
+ * stage timeline is on, blocks launch directly. */
+int fcw_engine_graphs(fcw_engine* e, int enable);
+
 /* Stage timeline: enable (1) / disable (0) CUDA-event marks between pipeline
  * stages on the working stream and reset the accumulated times and launch count. */
 int fcw_engine_profile(fcw_engine* e, int enable);

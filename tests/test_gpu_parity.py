@@ -201,6 +201,27 @@ def test_full_blocks_every_column_tile(precision, tol):
     assert np.max(err) <= tol, err
 
 
+def test_graph_replay_matches_direct_launches():
+    """Blocks replayed from each workspace's captured launch chain give the records of direct launches."""
+    z = _golden("golden_metrics_L5.npz")
+    pm = z["pm"]
+    src = pm.bfs[np.linspace(0, pm.n_vertices - 1, 300).astype(int)]
+    recs = []
+    for graphs in (False, True):
+        eng = engine.HeatEngine(pm.V, pm.F, block_k=64, pipeline_depth=2)
+        try:
+            eng.graphs(graphs)
+            for _ in range(2 if graphs else 1):  # the second call replays the first call's graphs
+                recs.append(eng.compute_metrics(src, z["targets"], n_between=3, precision="mixed"))
+        finally:
+            eng.close()
+    a = recs[0]
+    for b in recs[1:]:
+        both_nan = np.isnan(a) & np.isnan(b)
+        rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+        assert np.all(both_nan | (rel <= 1e-12))
+
+
 def test_pipelined_blocks_match_single_stream():
     """Several blocks in flight on separate streams give the same records as one stream."""
     z = _golden("golden_metrics_L5.npz")
