@@ -551,7 +551,7 @@ def main(argv=None):
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="L7")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--batch", type=int, default=4096, help="sources per step")
+    ap.add_argument("--batch", type=int, default=16384, help="sources per step")
     ap.add_argument("--block-k", type=int, default=1024)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--pipeline-depth", type=int, default=4, help="blocks in flight on separate streams")

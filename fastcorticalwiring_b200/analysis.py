@@ -33,7 +33,7 @@ class WiringAnalysis:
     DEFAULT_SCALES = (0.0006, 0.001, 0.002, 0.004, 0.008, 0.016)
 
     def __init__(self, vertices, faces, cortex_mask, engine_kwargs=None, eps=1e-6, precision="mixed",
-                 block_sources=8192):
+                 block_sources=16384):
         self.mesh = M.prepare(vertices, faces, cortex_mask)
         pm = self.mesh
         self.distance_engine = B200DistanceEngine(pm.V, pm.F, **dict(engine_kwargs or {}))
