@@ -180,19 +180,17 @@ __device__ __forceinline__ void face_cdf(double d0, double d1, double d2, double
     if (lo > mi) { t = lo; lo = mi; mi = t; }
     if (mi > hi) { t = mi; mi = hi; hi = t; }
     if (lo > mi) { t = lo; lo = mi; mi = t; }
-    if (r >= hi) { ar = A; da = 0.0; return; }
-    if (r <= lo) { ar = 0.0; da = 0.0; return; }
-    if (r < mi) {
-        const double den = (mi - lo) * (hi - lo);
-        const double x = r - lo;
-        ar = A * x * x / den;
-        da = 2.0 * A * x / den;
-        return;
-    }
-    const double den = (hi - lo) * (hi - mi);
-    const double y = hi - r;
-    ar = A * (1.0 - y * y / den);
-    da = 2.0 * A * y / den;
+    // both partial cases in one branch-free form (one division): x = r - lo below the
+    // middle corner, y = hi - r from it on
+    const bool below = r < mi;
+    const double z = below ? r - lo : hi - r;
+    const double q = z / ((hi - lo) * (below ? mi - lo : hi - mi));
+    const double zq = z * q;
+    const double a_in = below ? A * zq : A * (1.0 - zq);
+    const double d_in = 2.0 * A * q;
+    const bool whole = r >= hi, none = r <= lo;
+    ar = whole ? A : (none ? 0.0 : a_in);
+    da = (whole || none) ? 0.0 : d_in;
 }
 
 // |grad d| on a face (lean_geometry.py:91-96).
@@ -322,20 +320,20 @@ struct Field {
             // sub-bin j's faces are band[ptr[j-1], ptr[j]) after the counting sort
             int j = (j0 > 0 ? s->ptr[j0 - 1] : 0) + lane;
             const int je = s->ptr[j1 - 1];
-            // four records per lane in flight
-            for (; j + 96 < je; j += 128) {
-                int4 q[4];
-                double dd[4][3];
+            // two records per lane in flight
+            for (; j + 32 < je; j += 64) {
+                int4 q[2];
+                double dd[2][3];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) q[u] = band[j + 32 * u];
+                for (int u = 0; u < 2; ++u) q[u] = band[j + 32 * u];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < 2; ++u) {
                     dd[u][0] = dv(q[u].y);
                     dd[u][1] = dv(q[u].z);
                     dd[u][2] = dv(q[u].w);
                 }
 #pragma unroll
-                for (int u = 0; u < 4; ++u) rec_term(q[u], dd[u][0], dd[u][1], dd[u][2], r, mode, x1, x2);
+                for (int u = 0; u < 2; ++u) rec_term(q[u], dd[u][0], dd[u][1], dd[u][2], r, mode, x1, x2);
             }
             for (; j < je; j += 32) {
                 const int4 q0 = band[j];
