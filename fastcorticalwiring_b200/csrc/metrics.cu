@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs
                         const double d0 = (double)dd[u][0], d1 = (double)dd[u][1], d2 = (double)dd[u][2];
                         if (c >= 1 && d0 < R) continue;   // an earlier corner emits it
                         if (c == 2 && d1 < R) continue;
-                        if (!(isfinite(d0) && isfinite(d1) && isfinite(d2))) continue;
+                        // (every value is finite here: a field with a non-finite value is flagged above)
                         double lo = d0, hi = d0;
                         if (d1 < lo) lo = d1;
                         if (d1 > hi) hi = d1;
