@@ -48,7 +48,9 @@ enum { P_SUM_D, P_SUM_DA, P_SUM_A, P_CNT, P_NEG, P_VIOL, P_NONFINITE, P_DMAX, P_
 // counts of d < -h and of d < 0.9 |x - x_s| - h, the valid-distance sums and the maximum.
 // The chord test compares squares and takes the reference's sqrt form only within a
 // 1e-10 band of the threshold, so the counts match the reference exactly. Vertices
-// closer than the near radius are appended to their source's near list.
+// closer than the near radius are appended to their source's near list: per tile and
+// source, one atomic reserves the run, written in vertex order (which keeps the
+// per-source kernel's near-vertex walk local).
 template <typename Tin, typename Tout>
 __global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K, const Tin* __restrict__ phi,
                                                      Tout* __restrict__ dT) {
@@ -56,10 +58,12 @@ __global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K,
     __shared__ Tin sh[32];
     __shared__ double sc[32][3];
     __shared__ int srcv[32];
+    __shared__ unsigned nearmask[32][kStatVTile / 32];  // per source and sub-tile: lanes (vertices) near it
     const int n = a.n;
     const int k0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int vbase = blockIdx.x * kStatVTile;
+    nearmask[tx][ty] = 0u;  // (32 x 8 threads, one entry each)
     if (ty == 0) {
         const int sidx = a.src[k0 + tx];
         srcv[tx] = sidx;
@@ -139,12 +143,7 @@ __global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K,
                 }
             }
             const unsigned mask = __ballot_sync(0xffffffffu, near);
-            if (mask) {
-                int base = 0;
-                if (tx == 0) base = atomicAdd(&a.near_count[k], __popc(mask));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (near) a.near_list[(int64_t)k * n + base + __popc(mask & lanes_below)] = v;
-            }
+            if (tx == 0) nearmask[r][sub] = mask;
         }
     }
     // reduce over the 32 vertices of each warp (lanes), one source per (warp, j)
@@ -165,6 +164,32 @@ __global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K,
             double* q = a.partials + ((int64_t)blockIdx.x * K + k) * P_N;
             q[P_SUM_D] = sd[j]; q[P_SUM_DA] = sda[j]; q[P_SUM_A] = sa[j]; q[P_CNT] = (double)cnt[j];
             q[P_NEG] = (double)ng[j]; q[P_VIOL] = (double)vi[j]; q[P_NONFINITE] = (double)nf[j]; q[P_DMAX] = dm[j];
+        }
+    }
+    // the tile's near vertices of each source, appended to its list with one atomic, in vertex order
+    __syncthreads();
+    constexpr int NS = kStatVTile / 32;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int r = ty + 8 * j, k = k0 + r;
+        const unsigned m_l = tx < NS ? nearmask[r][tx] : 0u;
+        int c = __popc(m_l), incl = c;
+        for (int off = 1; off < NS; off <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, off);
+            if (tx >= off) incl += t;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, NS - 1);
+        if (total == 0) continue;  // warp-uniform
+        int base = 0;
+        if (tx == 0) base = atomicAdd(&a.near_count[k], total);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const int excl = incl - c;
+#pragma unroll
+        for (int sb = 0; sb < NS; ++sb) {
+            const unsigned m = nearmask[r][sb];
+            const int off = __shfl_sync(0xffffffffu, excl, sb);
+            if (m & (1u << tx))
+                a.near_list[(int64_t)k * n + base + off + __popc(m & lanes_below)] = vbase + sb * 32 + tx;
         }
     }
 }
