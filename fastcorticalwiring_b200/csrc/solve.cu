@@ -202,6 +202,53 @@ struct AccScalar {
         }
     }
 
+    // A lower triangular (row-major, zeros above the diagonal): depth block q of 16 reaches
+    // only the row blocks a >= q; the skipped products are exact zeros.
+    template <int MA>
+    __device__ __forceinline__ void rows_lower_n(const T* A, int lda, const T* Bm, int ldb, int depth) {
+        const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+        const T* ap = A + ty * lda;
+        const T* bp = Bm + G * tx;
+#pragma unroll
+        for (int q = 0; q < MA; ++q) {
+            const int j1 = min(depth, 16 * q + 16);
+            for (int j = 16 * q; j < j1; ++j) {
+                T w[NB];
+#pragma unroll
+                for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
+#pragma unroll
+                for (int a = q; a < MA; ++a) {
+                    const T l = ap[16 * a * lda + j];
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) c[a][b] += l * w[b];
+                }
+            }
+        }
+    }
+
+    // A read transposed (A[k*lda + i]) from a lower-triangular block: row i needs depth
+    // k >= i, so depth block q reaches only the row blocks a <= q.
+    template <int MA>
+    __device__ __forceinline__ void cols_upper_n(const T* A, int lda, const T* Bm, int ldb, int depth) {
+        const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+        const T* bp = Bm + G * tx;
+#pragma unroll
+        for (int q = 0; q < MA; ++q) {
+            const int j1 = min(depth, 16 * q + 16);
+            for (int j = 16 * q; j < j1; ++j) {
+                T w[NB], l[MA];
+#pragma unroll
+                for (int h = 0; h < NB / G; ++h) ldv(bp + j * ldb + 16 * G * h, &w[G * h]);
+#pragma unroll
+                for (int a = 0; a <= q; ++a) l[a] = A[j * lda + ty + 16 * a];
+#pragma unroll
+                for (int a = 0; a <= q; ++a)
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) c[a][b] += l[a] * w[b];
+            }
+        }
+    }
+
     // only the 16-row blocks holding one of the first nrows rows are computed
     __device__ __forceinline__ void rows(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
         const int na = (nrows + 15) >> 4;
@@ -210,6 +257,15 @@ struct AccScalar {
     __device__ __forceinline__ void cols(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
         const int na = (nrows + 15) >> 4;
         if (na > 0) upto<NA>(na, [&](auto m) { cols_n<decltype(m)::value>(A, lda, Bm, ldb, depth); });
+    }
+    // square triangular products (depth <= 16 * row blocks)
+    __device__ __forceinline__ void rows_lower(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
+        const int na = (nrows + 15) >> 4;
+        if (na > 0) upto<NA>(na, [&](auto m) { rows_lower_n<decltype(m)::value>(A, lda, Bm, ldb, depth); });
+    }
+    __device__ __forceinline__ void cols_upper(const T* A, int lda, const T* Bm, int ldb, int depth, int nrows) {
+        const int na = (nrows + 15) >> 4;
+        if (na > 0) upto<NA>(na, [&](auto m) { cols_upper_n<decltype(m)::value>(A, lda, Bm, ldb, depth); });
     }
 
     template <class F>
@@ -264,6 +320,38 @@ struct AccDmma {
                 mma(c[m], a, b);
             }
         }
+    }
+
+    // Triangular A (lower, zeros above the diagonal): depth steps [8q, 8q+8) reach the row
+    // tiles m >= q (row-major: rows need k <= row) or m <= q (transposed: k >= row).
+    template <int MM, bool TRANS>
+    __device__ __forceinline__ void run_tri(const double* A, int lda, const double* Bm, int ldb, int depth) {
+        const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, n0 = 8 * (threadIdx.x >> 5);
+        const double* bp = Bm + t * ldb + n0 + g;
+#pragma unroll
+        for (int q = 0; q < MM; ++q) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int k = 8 * q + 4 * h;
+                if (k >= depth) break;
+                const double b = bp[k * ldb];
+#pragma unroll
+                for (int m = TRANS ? 0 : q; m < (TRANS ? q + 1 : MM); ++m) {
+                    const double a = TRANS ? A[(k + t) * lda + 8 * m + g] : A[(8 * m + g) * lda + k + t];
+                    mma(c[m], a, b);
+                }
+            }
+        }
+    }
+    __device__ __forceinline__ void rows_lower(const double* A, int lda, const double* Bm, int ldb, int depth,
+                                               int nrows) {
+        const int nm = (nrows + 7) >> 3;
+        if (nm > 0) upto<MT>(nm, [&](auto m) { run_tri<decltype(m)::value, false>(A, lda, Bm, ldb, depth); });
+    }
+    __device__ __forceinline__ void cols_upper(const double* A, int lda, const double* Bm, int ldb, int depth,
+                                               int nrows) {
+        const int nm = (nrows + 7) >> 3;
+        if (nm > 0) upto<MT>(nm, [&](auto m) { run_tri<decltype(m)::value, true>(A, lda, Bm, ldb, depth); });
     }
 
     template <bool TRANS>
@@ -496,7 +584,7 @@ __global__ void __launch_bounds__(NT, 3) k_fwd(SolveArgs<T> a, int32_t t0) {
     AccT acc;
     if (want_x) {  // X = inv(L_ss) W, straight from the registers to B
         acc.zero();
-        acc.rows(Li, LA, Wt, LW, nsp, ns);
+        acc.rows_lower(Li, LA, Wt, LW, nsp, ns);
         T* xb = a.B + (int64_t)c0 * K + k0;
         acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(xb + (int64_t)r * K + c, v); });
     }
@@ -624,7 +712,7 @@ __global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
         }
         copy_async_wait();
         __syncthreads();
-        acc.cols(Ms, LA, Ys, LW, nsp, ns);
+        acc.cols_upper(Ms, LA, Ys, LW, nsp, ns);
     }
     T* out = a.B + (int64_t)c0 * K + k0;
     acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(out + (int64_t)r * K + c, v); });
