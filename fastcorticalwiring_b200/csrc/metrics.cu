@@ -43,7 +43,7 @@ __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a,
 // Per-(vertex tile, source) partial statistics written by k_shift_stats.
 enum { P_SUM_D, P_SUM_DA, P_SUM_A, P_CNT, P_NEG, P_VIOL, P_NONFINITE, P_DMAX, P_N };
 
-// The shift + transpose of one 256-vertex x 32-source tile, fused with the per-vertex
+// The shift + transpose of one kStatVTile-vertex x 32-source tile, fused with the per-vertex
 // work of the health screen and MSD (lean_geometry.py:343-357, core_analysis.py:1573-1581):
 // counts of d < -h and of d < 0.9 |x - x_s| - h, the valid-distance sums and the maximum.
 // The chord test compares squares and takes the reference's sqrt form only within a
@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K,
     const int k0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int vbase = blockIdx.x * kStatVTile;
-    nearmask[tx][ty] = 0u;  // (32 x 8 threads, one entry each)
+    for (int q = ty; q < kStatVTile / 32; q += 8) nearmask[tx][q] = 0u;
     if (ty == 0) {
         const int sidx = a.src[k0 + tx];
         srcv[tx] = sidx;
