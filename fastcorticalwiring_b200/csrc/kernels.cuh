@@ -168,7 +168,7 @@ struct MetricArgs {
     int32_t* near_list = nullptr;       // K x n: vertices closer than near_radius, per source
     int32_t* near_count = nullptr;      // K
 };
-constexpr int kStatVTile = 512;   // vertices per shift-statistics CTA
+constexpr int kStatVTile = 1024;   // vertices per shift-statistics CTA
 
 // ---- per-source sample assembly (samples.cu) ----
 constexpr int kMaxSamples = kMaxTargets + (kMaxTargets - 1) * kMaxBetween;
