@@ -48,8 +48,8 @@ L2_BYTES = 126 * 1024 * 1024
 # command and the per-kernel table. Other configurations report null.
 NCU_TRAFFIC = {
     ("L7", 1024, "mixed"): {
-        "heat_fwd": 0.140e9, "heat_bwd": 2.714e9, "divergence": 2.098e9, "poisson_fwd": 2.942e9,
-        "poisson_bwd": 1.954e9, "shift": 1.288e9, "metrics": 1.859e9,
+        "heat_fwd": 0.141e9, "heat_bwd": 2.725e9, "divergence": 2.097e9, "poisson_fwd": 2.941e9,
+        "poisson_bwd": 1.954e9, "shift": 1.329e9, "metrics": 1.773e9,
     },
 }
 
