@@ -2,7 +2,7 @@
 """Generate the golden fixtures from the reference's own code.
 
 Run in a checkout where the FastCorticalWiring reference is importable
-(default /root/reference, or --reference PATH). The GPU box never runs this:
+(default /root/reference, or --reference PATH). The tests never run this:
 its outputs are committed next to it as small .npz files.
 
 Reference code run here, unmodified:
