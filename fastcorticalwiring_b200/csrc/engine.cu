@@ -1,4 +1,4 @@
-// Engine lifecycle, factorisation driver, the per-block pipeline and the C ABI.
+// Engine lifecycle, factorisation sequence, the per-block pipeline and the C ABI.
 //
 // One engine = one cortical submesh on one GPU. Creation prepares the mesh on
 // the host, runs the symbolic analysis, uploads the structure and factors the

@@ -1,7 +1,7 @@
 """CPU oracle for the all-sources heat-method path.
 
-TEST INFRASTRUCTURE ONLY: a restatement of the reference algorithm used as the
-checker for the CUDA engine. Only tests/, __graft_entry__.smoke() and
+TEST INFRASTRUCTURE ONLY: a restatement of the reference algorithm that the CUDA
+engine's results are compared with. Only tests/, __graft_entry__.smoke() and
 bench.py's CPU-baseline leg may import it; the product path never does.
 
 Parity is pinned against golden vectors produced by the reference's own code

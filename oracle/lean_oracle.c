@@ -2,7 +2,7 @@
  * CPU oracle for the per-source geometry and the fused divergence.
  *
  * TEST INFRASTRUCTURE ONLY. This file is a plain-C restatement of the
- * reference algorithm, used as the checker for the CUDA path: only tests/,
+ * reference algorithm, the CUDA path's results are compared with: only tests/,
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it. The
  * product never links or calls it.
  *

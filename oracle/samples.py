@@ -1,6 +1,6 @@
 """Per-vertex (radius, area) sample assembly -- CPU restatement for the tests.
 
-TEST INFRASTRUCTURE ONLY (the checker for the device assembly kernel).
+TEST INFRASTRUCTURE ONLY (what the device assembly kernel is compared with).
 
 Restates, from the reference's core_analysis.py:
   * FastCorticalWiringAnalysis.boundary_area_loss_fraction   (core_analysis.py:759-777)
