@@ -153,7 +153,7 @@ struct MetricArgs {
     double targets[kMaxTargets];
     double fracs[kMaxBetween];
     const int32_t* src = nullptr;       // elimination-order source per column
-    int4* band = nullptr;               // nsrc * nf scratch: near faces (face, corners) sorted by bin
+    int4* band = nullptr;               // nsrc * nf scratch: near faces (face, corners) sorted by sub-bin
     int32_t* longf = nullptr;           // nsrc * nf scratch: near long faces
     double* out = nullptr;              // nsrc * stride
     const BlockDesc* desc = nullptr;    // when set, the records go to desc->out instead

@@ -288,7 +288,7 @@ struct Field {
     const T* d;
     const MetricArgs* a;
     SrcShared* s;
-    const int4* band;      // near faces (face, corners) sorted by bin
+    const int4* band;      // near faces (face, corners) sorted by sub-bin
     const int32_t* longf;  // near faces whose distance extent exceeds the bin width
 
     __device__ double dv(int v) const { return (double)d[v]; }
