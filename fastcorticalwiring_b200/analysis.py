@@ -116,7 +116,20 @@ class WiringAnalysis:
         Arguments and validation follow core_analysis.py:1441-1500; area_tol, batch_size and
         verbose are accepted and ignored as there.
         """
-        scales = self.normalize_scales(scale)
+        scales, m, cap = self.run_arguments(scale, n_samples_between_scales, boundary_cap_fraction)
+        targets = self._reset(scales, m, cap)
+        order = self._sources(vertex_subset)
+        eng = self.distance_engine.engine
+        for b0 in range(0, order.size, self.block_sources):
+            sub = order[b0:b0 + self.block_sources]
+            rec = eng.compute_metrics(sub, targets, n_between=m, eps=self.eps, precision=self.precision)
+            self._absorb(sub, rec, eng.assemble_samples(rec, targets, n_between=m, boundary_cap=cap))
+        self._finish(order.size)
+
+    @classmethod
+    def run_arguments(cls, scale, n_samples_between_scales, boundary_cap_fraction):
+        """Validated (scales, n_between, cap) of a run (core_analysis.py:1441-1500)."""
+        scales = cls.normalize_scales(scale)
         m = int(n_samples_between_scales)
         if m < 0:
             raise ValueError("n_samples_between_scales must be >= 0.")
@@ -133,7 +146,11 @@ class WiringAnalysis:
             raise ValueError(f"at most {MAX_TARGETS} scales per run on this engine, got {len(scales)}")
         if m > MAX_BETWEEN:
             raise ValueError(f"n_samples_between_scales must be <= {MAX_BETWEEN} on this engine, got {m}")
+        return scales, m, cap
 
+    # -- the steps of compute_all_wiring_costs (also driven by runner.py) ------
+    def _reset(self, scales, m, cap):
+        """Fresh result arrays for a run; returns the target areas of the scales."""
         n = self.n_vertices_full
         self.active_scales = scales
         self.n_samples_between_scales = m
@@ -144,52 +161,51 @@ class WiringAnalysis:
         self.radius_function = {float(s): np.full(n, np.nan, dtype=np.float32) for s in scales}
         self.perimeter_function = {float(s): np.full(n, np.nan, dtype=np.float32) for s in scales}
         self.field_flag = np.zeros(n, dtype=np.uint8)
-
+        self._counts = np.zeros(n, dtype=np.int64)
+        self._rows = []
+        self._flagged = []
         total_area = float(np.sum(self.vertex_areas_sub))
-        targets = np.array([total_area * float(s) for s in scales], dtype=np.float64)
-        nt = len(scales)
-        order = self._sources(vertex_subset)
-        eng = self.distance_engine.engine
-        counts = np.zeros(n, dtype=np.int64)
-        rows_r, rows_a, rows_at = [], [], []
-        flagged = []
-        for b0 in range(0, order.size, self.block_sources):
-            sub = order[b0:b0 + self.block_sources]
-            orig = self.sub_to_orig[sub]
-            rec = eng.compute_metrics(sub, targets, n_between=m, eps=self.eps, precision=self.precision)
-            bad = rec[:, 5] != 0.0
-            ok = ~bad
-            self.field_flag[orig[bad]] = 1
-            flagged.extend(zip(orig[bad].tolist(), rec[bad, 3].tolist(), rec[bad, 4].tolist()))
-            good = orig[ok]
-            self.dist_to_boundary[good] = rec[ok, 2].astype(np.float32)
-            self.msd_unweighted[good] = rec[ok, 0].astype(np.float32)
-            self.msd_weighted[good] = rec[ok, 1].astype(np.float32)
-            for i, s in enumerate(scales):
-                self.radius_function[float(s)][good] = rec[ok, 7 + i].astype(np.float32)
-                self.perimeter_function[float(s)][good] = rec[ok, 7 + nt + i].astype(np.float32)
-            r, a, c = eng.assemble_samples(rec, targets, n_between=m, boundary_cap=cap)
-            counts[orig] = c
-            rows_r.append(r)
-            rows_a.append(a)
-            rows_at.append(orig)
+        return np.array([total_area * float(s) for s in scales], dtype=np.float64)
 
-        # CSR over the full mesh, rows in vertex order (core_analysis.py:1619-1632)
+    def _absorb(self, sub, rec, samples):
+        """Records of the cortical sources `sub` (and their assembled samples) into the arrays."""
+        nt = len(self.active_scales)
+        orig = self.sub_to_orig[sub]
+        bad = rec[:, 5] != 0.0
+        ok = ~bad
+        self.field_flag[orig[bad]] = 1
+        self._flagged.extend(zip(orig[bad].tolist(), rec[bad, 3].tolist(), rec[bad, 4].tolist()))
+        good = orig[ok]
+        self.dist_to_boundary[good] = rec[ok, 2].astype(np.float32)
+        self.msd_unweighted[good] = rec[ok, 0].astype(np.float32)
+        self.msd_weighted[good] = rec[ok, 1].astype(np.float32)
+        for i, s in enumerate(self.active_scales):
+            self.radius_function[float(s)][good] = rec[ok, 7 + i].astype(np.float32)
+            self.perimeter_function[float(s)][good] = rec[ok, 7 + nt + i].astype(np.float32)
+        r, a, c = samples
+        self._counts[orig] = c
+        self._rows.append((r, a, orig))
+
+    def _finish(self, n_sources):
+        """The sample CSR over the full mesh, rows in vertex order (core_analysis.py:1619-1632)."""
+        n = self.n_vertices_full
+        counts = self._counts
         self.sample_indptr = np.zeros(n + 1, dtype=np.int64)
         np.cumsum(counts, out=self.sample_indptr[1:])
         total = int(self.sample_indptr[-1])
         self.sample_radii_flat = np.empty(total, dtype=np.float32)
         self.sample_areas_flat = np.empty(total, dtype=np.float32)
-        for r, a, orig in zip(rows_r, rows_a, rows_at):
+        for r, a, orig in self._rows:
             c = counts[orig]
             used = np.arange(r.shape[1])[None, :] < c[:, None]
             dst = (self.sample_indptr[orig][:, None] + np.arange(r.shape[1])[None, :])[used]
             self.sample_radii_flat[dst] = r[used]
             self.sample_areas_flat[dst] = a[used]
-
+        flagged = self._flagged
+        self._counts, self._rows, self._flagged = None, None, None
         self.n_flagged_fields = len(flagged)
         if flagged:
-            msg = (f"{len(flagged)} of {order.size} source vertices had corrupted distance fields; "
+            msg = (f"{len(flagged)} of {n_sources} source vertices had corrupted distance fields; "
                    "all metrics for them were set to NaN (see field_flag).")
             warnings.warn(msg, RuntimeWarning)
 

@@ -150,6 +150,33 @@ def _precision(p) -> int:
     raise ValueError(f"precision must be 'fp64' or 'mixed', got {p!r}")
 
 
+def assemble_samples_device(records, targets, n_between=3, boundary_cap=None, device=0):
+    """fcw_assemble_samples_device on host records, without an engine: the records go to
+    `device`, the (radii, areas, counts) rows come back (as HeatEngine.assemble_samples)."""
+    import torch
+
+    rec = np.ascontiguousarray(records, dtype=np.float64)
+    t = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1)
+    n = rec.shape[0]
+    cap = _lib.samples_capacity(t.size, n_between)
+    if n == 0:
+        return (np.empty((0, cap), np.float32), np.empty((0, cap), np.float32), np.empty(0, np.int32))
+    dev = f"cuda:{int(device)}"
+    with torch.cuda.device(dev):
+        rec_d = torch.from_numpy(rec).to(dev)
+        radii = torch.empty((n, cap), dtype=torch.float32, device=dev)
+        areas = torch.empty((n, cap), dtype=torch.float32, device=dev)
+        counts = torch.empty(n, dtype=torch.int32, device=dev)
+        stream = torch.cuda.current_stream()
+        c = float("nan") if boundary_cap is None else float(boundary_cap)
+        _lib.check(_lib.load().fcw_assemble_samples_device(
+            ctypes.c_void_p(rec_d.data_ptr()), n, t.size, int(n_between), _lib.ptr(t), c,
+            ctypes.c_void_p(radii.data_ptr()), ctypes.c_void_p(areas.data_ptr()), ctypes.c_void_p(counts.data_ptr()),
+            ctypes.c_void_p(stream.cuda_stream)))
+        stream.synchronize()
+        return radii.cpu().numpy(), areas.cpu().numpy(), counts.cpu().numpy()
+
+
 def split_records(rec: np.ndarray, n_targets: int, n_between: int) -> dict:
     """Named views of raw records (n, stride)."""
     ne = max(0, n_targets - 1) * n_between

@@ -40,6 +40,7 @@ class Job:
     sources: np.ndarray | None = None  # cortical sub-indices; None = all, in BFS order
     precision: str = "mixed"
     eps: float = 1e-6
+    prepared: M.PreparedMesh | None = None  # the mesh already prepared on the host (else done on admission)
 
 
 @dataclass
@@ -53,6 +54,7 @@ class JobResult:
     device_bytes: int
     n_vertices: int
     estimate_bytes: int = 0
+    engine_info: dict | None = None
 
     @property
     def latency_s(self) -> float:
@@ -204,11 +206,12 @@ class Server:
         a.eng.synchronize(a.stream.cuda_stream)  # surfaces kernel error flags
         rec = a.out_dev.cpu().numpy()
         t_done = time.perf_counter()
-        info_bytes = int(a.eng.info()["device_bytes"])
+        info = a.eng.info()
+        info_bytes = int(info["device_bytes"])
         a.eng.close()
         a.src_dev = a.out_dev = None  # back to the tensor cache; no device-wide free
         res = JobResult(a.job.job_id, a.sources, rec, a.t_arrive, a.t_admit, t_done, info_bytes,
-                        int(a.sources.size), a.estimate)
+                        int(a.sources.size), a.estimate, info)
         with self._cv:
             self.results[a.job.job_id] = res
             self._reserved -= a.reserved
@@ -278,7 +281,7 @@ class Server:
     def _admit(self, p: _Pending) -> _Active:
         torch = self.torch
         job = p.job
-        pm = M.prepare(job.vertices, job.faces, job.cortex_mask)
+        pm = job.prepared if job.prepared is not None else M.prepare(job.vertices, job.faces, job.cortex_mask)
         eng = E.HeatEngine(pm.V, pm.F, device=self.device, **self.params)
         src = pm.bfs.astype(np.int32) if job.sources is None else np.asarray(job.sources, dtype=np.int32)
         targets = pm.targets(job.scales)
