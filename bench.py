@@ -44,8 +44,10 @@ L2_BYTES = 126 * 1024 * 1024
 
 # DRAM bytes (read + write) per 1024-source block of each stage on the L7 mixed
 # workload, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum
-# summed over the stage's launches); profiles/dram_L7_block1024_mixed.md has the
-# command and the per-kernel table. Other configurations report null.
+# summed over the stage's launches, divided by the 8 blocks of the process) of
+#   python bench.py --workload L7 --batch 1024 --steps 1 --warmup 3 --cpu-sample 0
+#       --quick --pipeline-depth 1
+# Other configurations report null.
 NCU_TRAFFIC = {
     ("L7", 1024, "mixed"): {
         "heat_fwd": 0.141e9, "heat_bwd": 2.725e9, "divergence": 2.097e9, "poisson_fwd": 2.941e9,
