@@ -140,6 +140,38 @@ def _analysis_fixture(ca, lg, fl, mesh, n_sources, with_stages):
     return out
 
 
+def _params_fixture(ca, mesh, n_sources, diffusion_length_mm, n_between):
+    """The analysis with non-default settings: diffusion length, the default scales, n_between."""
+    with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()):
+        an = ca.FastCorticalWiringAnalysis(mesh.vertices, mesh.faces, mesh.cortex_mask,
+                                           engine_type="consistent_heat_reference",
+                                           engine_kwargs={"diffusion_length_mm": diffusion_length_mm})
+    order = np.asarray(an._bfs_order)
+    pick = order[np.linspace(0, order.size - 1, n_sources).astype(int)]
+    subset = an.sub_to_orig[pick]
+    with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()), \
+            warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        an.compute_all_wiring_costs(scale=None, vertex_subset=subset, n_samples_between_scales=n_between)
+    out = dict(V=mesh.vertices, F=mesh.faces, mask=mesh.cortex_mask, level=mesh.level, seed=mesh.seed,
+               jitter=mesh.jitter, diffusion_length_mm=float(diffusion_length_mm), n_between=int(n_between),
+               scales=np.asarray(ca.FastCorticalWiringAnalysis.DEFAULT_SCALES, dtype=np.float64),
+               sources_orig=subset.astype(np.int64), t=an.distance_engine._eng.t)
+    for k, v in an.get_metric_arrays().items():
+        out["f32_" + k] = v[subset]
+    out["field_flag"] = an.field_flag[subset]
+    indptr, rs, as_ = [0], [], []
+    for o in subset:
+        r, a = an.get_vertex_samples(int(o))
+        rs.append(r)
+        as_.append(a)
+        indptr.append(indptr[-1] + r.size)
+    out["sample_indptr"] = np.asarray(indptr, np.int64)
+    out["sample_r"] = np.concatenate(rs).astype(np.float32)
+    out["sample_a"] = np.concatenate(as_).astype(np.float32)
+    return out
+
+
 def _samples_fixture(ca, lg, mesh, n_sources, cap):
     import io_utils as iu  # noqa: E402  (the reference's writer)
     import tempfile
@@ -285,6 +317,7 @@ def main():
     ca, de, fl, lg, tk = _ref_modules(args.reference)
     l4 = folded_icosphere(4, seed=11, jitter=0.2)
     l5 = folded_icosphere(5, seed=5)
+    l4b = folded_icosphere(4, seed=21, jitter=0.3)
 
     def metrics_l5():
         fx = _analysis_fixture(ca, lg, fl, l5, 16, False)
@@ -296,6 +329,7 @@ def main():
         "golden_metrics_L5.npz": metrics_l5,
         "golden_geometry_kat.npz": lambda: _geometry_kat(ca, lg, tk),
         "golden_samples_L5.npz": lambda: _samples_fixture(ca, lg, l5, 24, 0.05),
+        "golden_params_L4.npz": lambda: _params_fixture(ca, l4b, 12, 1.0, 1),
     }
     for name, make in fixtures.items():
         if args.only and name != args.only:

@@ -89,6 +89,29 @@ def test_oracle_analysis_outputs_match_reference_float32(fx):
             np.testing.assert_allclose(np.float32(out["perim"][i]), fx["f32_perimeter_" + tok][j], rtol=2.4e-7)
 
 
+def test_oracle_matches_reference_with_other_settings():
+    """Diffusion length 1.0 mm, the analysis' default six scales and one sample between scales."""
+    z = _load("golden_params_L4.npz")
+    pm = M.prepare(z["V"], z["F"], z["mask"])
+    ho = oracle.HeatOracle(pm.V, pm.F, diffusion_length_mm=float(z["diffusion_length_mm"]))
+    assert ho.t == float(z["t"])
+    sub = pm.orig_to_sub[z["sources_orig"]]
+    phi = ho.distances(sub)
+    targets = pm.targets(z["scales"])
+    nb = int(z["n_between"])
+    for j, s in enumerate(sub):
+        out = oracle.source_metrics(phi[j], int(s), pm, targets, n_between=nb)
+        assert out["bad"] == bool(z["field_flag"][j])
+        for i, sc in enumerate(z["scales"]):
+            tok = format(float(sc), "g")
+            # FP64 fields from two factorisations differ at 1e-15: allow one float32 ulp
+            np.testing.assert_allclose(np.float32(out["radii"][i]), z[f"f32_radius_{tok}"][j], rtol=2.4e-7)
+            np.testing.assert_allclose(np.float32(out["perim"][i]), z[f"f32_perimeter_{tok}"][j], rtol=2.4e-7)
+        np.testing.assert_allclose(np.float32(out["msd_w"]), z["f32_msd_weighted"][j], rtol=2.4e-7)
+        lo, hi = z["sample_indptr"][j], z["sample_indptr"][j + 1]
+        assert hi - lo == len(z["scales"]) + (len(z["scales"]) - 1) * nb
+
+
 def test_geometry_kat():
     z = _load("golden_geometry_kat.npz")
     V, F = z["V"], z["F"].astype(np.int32)
