@@ -128,6 +128,31 @@ def test_geometry_on_reference_fields(l4):
     assert np.array_equal(np.float32(r["dist_b"]), l4["f32_dist_to_boundary"])
 
 
+def test_most_targets_and_samples_on_reference_fields(l4):
+    """32 scales with 8 samples between each pair (the engine's maximum) on the reference's own
+    fields, against the oracle's geometry; one more of either is rejected at the boundary, and an
+    empty source list gives an empty result."""
+    import oracle
+
+    pm, eng = l4["pm"], l4["eng"]
+    scales = np.geomspace(0.001, 0.08, 32)
+    targets = pm.targets(scales)
+    fr = np.arange(1, 9) / 9.0
+    r = _field_metrics(eng, l4["phi"], l4["sources_sub"], targets, n_between=8)
+    for j in range(l4["phi"].shape[0]):
+        rad, per, er, ea, _ = oracle.source_geometry(l4["phi"][j], pm.F, pm.lean_area, pm.g11, pm.g12, pm.g22,
+                                                     pm.bin_width, targets, fr)
+        for got, ref in ((r["radii"][j], rad), (r["perim"][j], per), (r["extra_r"][j], er), (r["extra_a"][j], ea)):
+            both = np.isnan(got) & np.isnan(ref)
+            assert np.all(both | (_rel(got, ref) <= 1e-12))
+    with pytest.raises(_lib.FCWError):
+        eng.compute_metrics(l4["sources_sub"][:2], pm.targets(np.geomspace(0.001, 0.08, 33)), n_between=3)
+    with pytest.raises(_lib.FCWError):
+        eng.compute_metrics(l4["sources_sub"][:2], targets, n_between=9)
+    empty = eng.compute_metrics(np.zeros(0, np.int32), targets, n_between=8)
+    assert empty.shape == (0, _lib.metrics_stride(32, 8))
+
+
 def test_geometry_kat_fields_long_faces_and_nan_rules():
     z = dict(np.load(os.path.join(GOLDEN, "golden_geometry_kat.npz")))
     V, F = z["V"], z["F"].astype(np.int32)
