@@ -153,6 +153,33 @@ def test_most_targets_and_samples_on_reference_fields(l4):
     assert empty.shape == (0, _lib.metrics_stride(32, 8))
 
 
+@pytest.mark.parametrize("precision, tol", [("fp64", 1e-9), ("mixed", 1e-4)])
+def test_closed_surface_without_boundary(precision, tol):
+    """A closed surface (no boundary vertices): distance to boundary is +inf (core_analysis.py:1566-1572)
+    and the rest matches the oracle."""
+    import oracle
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    m = folded_icosphere(4, seed=2, jitter=0.2)
+    pm = M.prepare(m.vertices, m.faces, np.ones(len(m.vertices), bool))
+    assert pm.boundary.size == 0
+    src = pm.bfs[np.linspace(0, pm.n_vertices - 1, 6).astype(int)]
+    targets = pm.targets(SCALES)
+    eng = engine.HeatEngine(pm.V, pm.F)
+    try:
+        r = engine.split_records(eng.compute_metrics(src, targets, 3, precision=precision), len(SCALES), 3)
+    finally:
+        eng.close()
+    assert np.all(np.isposinf(r["dist_b"]))
+    phi = oracle.HeatOracle(pm.V, pm.F).distances(src)
+    for j, s in enumerate(src):
+        ref = oracle.source_metrics(phi[j], int(s), pm, targets)
+        assert bool(r["bad"][j]) == ref["bad"]
+        assert np.max(_rel(r["radii"][j], ref["radii"])) <= tol
+        assert np.max(_rel(r["perim"][j], ref["perim"])) <= tol
+        assert abs(r["msd_w"][j] - ref["msd_w"]) <= tol * ref["msd_w"]
+
+
 def test_geometry_kat_fields_long_faces_and_nan_rules():
     z = dict(np.load(os.path.join(GOLDEN, "golden_geometry_kat.npz")))
     V, F = z["V"], z["F"].astype(np.int32)
