@@ -180,6 +180,33 @@ def test_closed_surface_without_boundary(precision, tol):
         assert abs(r["msd_w"][j] - ref["msd_w"]) <= tol * ref["msd_w"]
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sphere_against_closed_forms(precision):
+    """Analytic check in the spirit of the reference's validate_fastcw_pp3d.py (sphere closed
+    forms, radius 3-5% and perimeter 2-3% there): on a 70 mm order-6 icosphere the geodesic disc
+    holding area A has radius R acos(1 - A / (2 pi R^2)) and perimeter 2 pi R sin(r / R). The heat
+    method at 0.7 mm is biased by a few percent in radius (and much less in perimeter)."""
+    from fastcorticalwiring_b200.meshgen import unit_icosphere
+
+    R = 70.0
+    V, F = unit_icosphere(6)
+    pm = M.prepare(V * R, F, np.ones(len(V), bool))
+    scales = np.array([0.002, 0.01, 0.05, 0.2])
+    targets = pm.targets(scales)
+    src = pm.bfs[np.linspace(0, pm.n_vertices - 1, 8).astype(int)]
+    eng = engine.HeatEngine(pm.V, pm.F)
+    try:
+        r = engine.split_records(eng.compute_metrics(src, targets, 3, precision=precision), scales.size, 3)
+    finally:
+        eng.close()
+    assert not r["bad"].any()
+    frac = targets / (4.0 * np.pi * R * R)  # of the smooth sphere's area
+    r_cf = R * np.arccos(1.0 - 2.0 * frac)
+    p_cf = 2.0 * np.pi * R * np.sin(r_cf / R)
+    assert np.max(np.abs(r["radii"] - r_cf) / r_cf) <= 0.04
+    assert np.max(np.abs(r["perim"] - p_cf) / p_cf) <= 0.02
+
+
 def test_geometry_kat_fields_long_faces_and_nan_rules():
     z = dict(np.load(os.path.join(GOLDEN, "golden_geometry_kat.npz")))
     V, F = z["V"], z["F"].astype(np.int32)
