@@ -112,3 +112,20 @@ def test_invalid_mesh_is_rejected_at_the_boundary():
     with pytest.raises(_lib.FCWError) as ei:
         _lib.analyze(V, np.array([[0, 1, 5]], dtype=np.int32))
     assert ei.value.code == _lib.FCW_E_INVALID and "out of range" in str(ei.value)
+
+
+def test_record_layout_matches_the_header():
+    """fcw_metrics_stride and the FCW_M_* offsets: 7 scalars, radii, perimeters, then the samples."""
+    for nt, nb in ((1, 0), (12, 3), (32, 8)):
+        ne = (nt - 1) * nb
+        stride = _lib.metrics_stride(nt, nb)
+        assert stride == 7 + 2 * nt + 2 * ne
+        rec = np.arange(2 * stride, dtype=np.float64).reshape(2, stride)
+        r = engine.split_records(rec, nt, nb)
+        assert r["msd_u"][1] == stride + _lib.M_MSD_U and r["dist_b"][0] == _lib.M_DIST_B
+        assert r["radii"].shape == (2, nt) and r["radii"][0, 0] == _lib.M_RADII
+        assert r["perim"][0, 0] == _lib.M_RADII + nt
+        assert r["extra_r"].shape == (2, ne) and r["extra_a"].shape == (2, ne)
+        if ne:
+            assert r["extra_a"][0, -1] == stride - 1
+    assert _lib.samples_capacity(32, 8) == 32 + 31 * 8
