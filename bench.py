@@ -252,6 +252,22 @@ def _stage_bytes(stage, n, nf, K, nnz_factor, precision, nreached_rows=None):
     return 0
 
 
+def shard_sources(order, world, rank):
+    """Rank `rank`'s contiguous slice of the BFS order: every source on exactly one rank."""
+    return np.array_split(np.asarray(order), world)[rank]
+
+
+def max_over_ranks(x, dist, device):
+    """The slowest rank's value, on every rank (a multi-rank time is the max over ranks)."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_gpu(args):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -294,7 +310,7 @@ def run_gpu(args):
     info = eng.info()
 
     bfs = pm.bfs.astype(np.int32)
-    share = np.array_split(bfs, world)[rank]
+    share = shard_sources(bfs, world, rank)
     B = args.batch
     stride = E._lib.metrics_stride(12, N_BETWEEN)
     src_dev = torch.from_numpy(share.copy()).to(f"cuda:{dev}")
@@ -349,10 +365,7 @@ def run_gpu(args):
     stages, _ = eng.stage_times()
     eng.profile(False)
     stages = {k: v / nprof for k, v in stages.items()}  # ms per block
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, f"cuda:{dev}")
     total_sources = B * args.steps * world
     value = total_sources / (ms / 1e3)
 
@@ -374,10 +387,7 @@ def run_gpu(args):
                                              E._lib.ptr(tgt), tgt.size, N_BETWEEN, 1e-6, E._lib.ptr(h_out)))
     e2e_s = time.perf_counter() - t0
     barrier()
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, f"cuda:{dev}")
     e2e = total_sources / e2e_s
 
     extra = {}
