@@ -311,7 +311,8 @@ def run_gpu(args):
 
     bfs = pm.bfs.astype(np.int32)
     share = shard_sources(bfs, world, rank)
-    B = args.batch
+    # a step never holds more sources than every rank's slice (the mesh may be smaller than a batch)
+    B = args.batch = min(args.batch, bfs.size // world)
     stride = E._lib.metrics_stride(12, N_BETWEEN)
     src_dev = torch.from_numpy(share.copy()).to(f"cuda:{dev}")
     out_dev = torch.empty((B, stride), dtype=torch.float64, device=f"cuda:{dev}")
