@@ -110,6 +110,9 @@ def run_subjects(subjects, output_dir, scale=None, n_samples_between_scales=3, b
     Returns {"written": {name: path}, "failed": {name: message}, "sources_per_s": ..., "jobs": [...]}.
     """
     scales, m, cap = A.WiringAnalysis.run_arguments(scale, n_samples_between_scales, boundary_cap_fraction)
+    names = [name for name, _ in subjects]
+    if len(set(names)) != len(names):
+        raise ValueError("subject names must be unique")
     log = log or (lambda msg: None)
     prepared, failed = {}, {}
     jobs = []

@@ -40,6 +40,11 @@ def test_unreadable_subjects_are_skipped_without_a_device(tmp_path):
     assert out["written"] == {} and "gone" in out["failed"]
 
 
+def test_duplicate_subject_names_are_rejected(tmp_path):
+    with pytest.raises(ValueError, match="unique"):
+        runner.run_subjects([("a", "x.npz"), ("a", "y.npz")], str(tmp_path))
+
+
 def test_run_arguments_follow_the_analysis_rules(tmp_path):
     with pytest.raises(ValueError, match="boundary_cap_fraction"):
         runner.run_subjects([], str(tmp_path), boundary_cap_fraction=0.5)
