@@ -26,16 +26,61 @@ MAX_TARGETS = 32                         # scales per run the device kernels hol
 MAX_BETWEEN = 8                          # supplementary samples per gap
 
 
+def classify_nonmanifold_vertices(vertices, faces):
+    """Boundary and non-manifold vertices of a triangle mesh (core_analysis.py:60-110).
+
+    Returns sets: boundary_verts (on an edge of one face), non_manifold_verts (on an
+    edge of more than two faces), also_boundary (both) and interior (non-manifold only).
+    """
+    V = np.asarray(vertices)
+    F = np.asarray(faces)
+    if V.ndim != 2 or V.shape[1] != 3:
+        raise ValueError(f"Invalid vertex array shape {V.shape}; expected (N, 3).")
+    if F.ndim != 2 or F.shape[1] != 3:
+        raise ValueError(f"Invalid face array shape {F.shape}; expected (M, 3).")
+    if F.size == 0:
+        return {"boundary_verts": set(), "non_manifold_verts": set(), "also_boundary": set(), "interior": set()}
+    e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]]).astype(np.int64)
+    e.sort(axis=1)
+    edges, counts = np.unique(e, axis=0, return_counts=True)
+    boundary = set(np.unique(edges[counts == 1]).tolist())
+    non_manifold = set(np.unique(edges[counts > 2]).tolist())
+    return {"boundary_verts": boundary, "non_manifold_verts": non_manifold,
+            "also_boundary": non_manifold & boundary, "interior": non_manifold - boundary}
+
+
 class WiringAnalysis:
-    """A cortical mesh, its B200 engine and the per-vertex wiring metrics."""
+    """A cortical mesh, its B200 engine and the per-vertex wiring metrics.
+
+    The constructor takes FastCorticalWiringAnalysis's arguments (core_analysis.py:545-586):
+    engine_type must name this engine ("b200"); metadata is kept; a cortical submesh with
+    interior non-manifold vertices warns unless allow_interior_nonmanifold, as the
+    reference does for engines without the robust operators (core_analysis.py:609-636).
+    precision and block_sources are this engine's own settings.
+    """
 
     # core_analysis.py:536-543
     DEFAULT_SCALES = (0.0006, 0.001, 0.002, 0.004, 0.008, 0.016)
 
-    def __init__(self, vertices, faces, cortex_mask, engine_kwargs=None, eps=1e-6, precision="mixed",
-                 block_sources=16384):
+    def __init__(self, vertices, faces, cortex_mask, engine_type="b200", engine_kwargs=None, eps=1e-6,
+                 metadata=None, allow_interior_nonmanifold=False, precision="mixed", block_sources=16384):
+        key = str(engine_type).strip().lower()
+        if key != "b200":
+            raise ValueError(f"Unknown engine_type '{engine_type}'. Valid options: b200")
+        self.engine_type = key
+        self.metadata = dict(metadata or {})
+        self.allow_interior_nonmanifold = bool(allow_interior_nonmanifold)
         self.mesh = M.prepare(vertices, faces, cortex_mask)
         pm = self.mesh
+        report = classify_nonmanifold_vertices(pm.V, pm.F)
+        self.n_interior_nonmanifold = len(report["interior"])
+        if self.n_interior_nonmanifold and not self.allow_interior_nonmanifold:
+            warnings.warn(
+                "Interior non-manifold vertices detected in cortical submesh. "
+                "Automatic use_robust fallback is only available for the potpourri engine; "
+                f"continuing with engine_type={self.engine_type!r}.",
+                RuntimeWarning,
+            )
         self.distance_engine = B200DistanceEngine(pm.V, pm.F, **dict(engine_kwargs or {}))
         self.eps = float(eps)
         self.precision = precision

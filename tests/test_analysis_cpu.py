@@ -59,3 +59,41 @@ def test_vertex_subset_filtering_and_order():
     assert list(got) == sorted(got, key=bfs.index)  # BFS order
     assert np.array_equal(wa._sources(None), pm.bfs)
     assert wa._sources([]).size == 0
+
+
+def test_nonmanifold_classification():
+    """core_analysis.py:60-110 on crafted meshes: one face has three boundary edges; a fan of
+    three faces on one edge makes both of its vertices non-manifold."""
+    V = np.zeros((6, 3))
+    r = A.classify_nonmanifold_vertices(V, np.array([[0, 1, 2]]))
+    assert r["boundary_verts"] == {0, 1, 2} and r["non_manifold_verts"] == set()
+    F = np.array([[0, 1, 2], [1, 0, 3], [0, 1, 4]])
+    r = A.classify_nonmanifold_vertices(V, F)
+    assert r["non_manifold_verts"] == {0, 1}
+    assert r["boundary_verts"] == {0, 1, 2, 3, 4} and r["also_boundary"] == {0, 1} and r["interior"] == set()
+    assert A.classify_nonmanifold_vertices(V, np.zeros((0, 3), int))["interior"] == set()
+    with pytest.raises(ValueError, match="expected \\(M, 3\\)"):
+        A.classify_nonmanifold_vertices(V, np.zeros((2, 4), int))
+
+
+def test_constructor_follows_the_reference():
+    """engine_type must name this engine; an interior non-manifold cortical submesh warns as the
+    reference does for engines without robust operators, before the engine is built."""
+    import torch
+
+    from fastcorticalwiring_b200 import _lib
+
+    mesh = folded_icosphere(3, seed=1)
+    with pytest.raises(ValueError, match="Unknown engine_type 'potpourri'"):
+        A.WiringAnalysis(mesh.vertices, mesh.faces, mesh.cortex_mask, engine_type="potpourri")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible: the engine would be built")
+    # a closed icosphere with a two-sided fin on an existing edge: an interior non-manifold edge
+    V, F = mesh.vertices, mesh.faces
+    a, b = F[0, 0], F[0, 1]
+    V2 = np.vstack([V, V[a] + 1.0])
+    F2 = np.vstack([F, [a, b, len(V)], [b, a, len(V)]])
+    assert A.classify_nonmanifold_vertices(V2, F2)["interior"] == {int(a), int(b)}
+    with pytest.warns(RuntimeWarning, match="Interior non-manifold vertices"):
+        with pytest.raises(_lib.FCWError):
+            A.WiringAnalysis(V2, F2, np.ones(len(V2), bool), metadata={"subject": "x"})
