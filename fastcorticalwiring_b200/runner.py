@@ -40,9 +40,11 @@ class SubjectAnalysis(A.WiringAnalysis):
     """WiringAnalysis results filled from a serving job's records (no engine of its own)."""
 
     def __init__(self, pm: M.PreparedMesh, engine_info: dict, diffusion_length_mm: float, eps=1e-6,
-                 precision="mixed"):
+                 precision="mixed", metadata=None):
         self.mesh = pm
         self.distance_engine = None
+        self.engine_type = "b200"
+        self.metadata = dict(metadata or {})
         self._engine_info = dict(engine_info or {})
         self._diffusion_length_mm = float(diffusion_length_mm)
         self.eps = float(eps)
@@ -142,7 +144,7 @@ def run_subjects(subjects, output_dir, scale=None, n_samples_between_scales=3, b
         diffusion = float(params.get("diffusion_length_mm", E.DEFAULT_DIFFUSION_LENGTH_MM))
         for name, pm in prepared.items():
             res = results[name]
-            sa = SubjectAnalysis(pm, res.engine_info, diffusion, precision=precision)
+            sa = SubjectAnalysis(pm, res.engine_info, diffusion, precision=precision, metadata={"subject": name})
             targets = sa._reset(scales, m, cap)
             sa._absorb(res.sources, res.records,
                        E.assemble_samples_device(res.records, targets, m, cap, device=device))
