@@ -52,3 +52,41 @@ def test_run_arguments_follow_the_analysis_rules(tmp_path):
         runner.run_subjects([], str(tmp_path), n_samples_between_scales=-1)
     with pytest.raises(SystemExit):
         runner.main(["--out", str(tmp_path)])  # no subjects
+
+
+def test_subject_analysis_from_records_writes_schema_v3(tmp_path):
+    """The runner's glue on the host: records and samples into the analysis arrays and the NPZ."""
+    from fastcorticalwiring_b200 import _lib, analysis, mesh as M
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    mesh = folded_icosphere(3, seed=4)
+    pm = M.prepare(mesh.vertices, mesh.faces, mesh.cortex_mask)
+    sa = runner.SubjectAnalysis(pm, {"t_coef": 2.0, "mean_edge_length": 0.5}, 0.7, metadata={"subject": "s"})
+    scales, m, cap = analysis.WiringAnalysis.run_arguments(None, 1, None)
+    targets = sa._reset(scales, m, cap)
+    assert np.allclose(targets, pm.targets(scales))
+    src = pm.bfs[:5].astype(np.int32)
+    nt = len(scales)
+    rec = np.zeros((src.size, _lib.metrics_stride(nt, m)))
+    rec[:, 0], rec[:, 1], rec[:, 2] = 10.0, 11.0, 3.0
+    rec[2, 5] = 1.0  # one flagged field
+    rec[:, 7:7 + nt] = np.arange(1, nt + 1)
+    cap_n = _lib.samples_capacity(nt, m)
+    radii = np.tile(np.arange(cap_n, dtype=np.float32), (src.size, 1))
+    counts = np.array([3, 0, 0, 1, 2], np.int32)
+    with pytest.warns(RuntimeWarning, match="1 of 5 source vertices"):
+        sa._absorb(src, rec, (radii, radii * 2, counts))
+        sa._finish(src.size)
+    orig = pm.sub_to_orig[src]
+    assert sa.field_flag[orig[2]] == 1 and np.isnan(sa.msd_weighted[orig[2]])
+    assert sa.msd_weighted[orig[0]] == np.float32(11.0)
+    assert sa.radius_function[scales[-1]][orig[1]] == np.float32(nt)
+    assert int(sa.sample_indptr[-1]) == int(counts.sum())
+    r, a = sa.get_vertex_samples(orig[0])
+    assert list(r) == [0.0, 1.0, 2.0] and list(a) == [0.0, 2.0, 4.0]
+    path = analysis.save_analysis_npz(str(tmp_path), "s.npz", sa)
+    z = np.load(path)
+    assert int(z["fastcw_output_schema_version"]) == 3 and int(z["n_samples_between_scales"]) == 1
+    prov = json.loads(str(z["provenance_json"]))
+    assert prov["engine"] == "b200" and prov["t_coef"] == 2.0 and prov["n_flagged_fields"] == 1
+    assert sa.metadata == {"subject": "s"}
