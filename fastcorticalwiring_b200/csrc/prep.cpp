@@ -156,41 +156,48 @@ int prepare_mesh(const double* V, int64_t nv, const int32_t* F, int64_t nf, Mesh
     for (int c = 0; c < 3; ++c)
         for (int64_t f = 0; f < nf; ++f) m.mass[F[3 * f + c]] += m.grad_area[f] / 3.0;
 
-    // Stiffness L = G^T diag(A) G as full symmetric CSC; duplicates summed in
-    // the order the reference concatenates its triplets (block (i,j), then face).
+    // Stiffness L = G^T diag(A) G as full symmetric CSC; duplicates summed in the
+    // order the reference concatenates its triplets (block (i,j), then face): the
+    // triplet (i, j, f) lands in column F[f][j], row F[f][i], at position
+    // (3i + j) nf + f of the reference's list. Column by column from the vertex's
+    // incident faces, entries sorted by (row, that position), so each row's
+    // duplicates add in the reference's order.
     {
-        std::vector<int64_t> cnt(nv + 1, 0);
-        for (int64_t f = 0; f < nf; ++f)
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) cnt[F[3 * f + j] + 1]++;
-        std::vector<int64_t> colptr(nv + 1, 0);
-        for (int64_t v = 0; v < nv; ++v) colptr[v + 1] = colptr[v] + cnt[v + 1];
-        std::vector<int64_t> fill(colptr.begin(), colptr.end() - 1);
-        std::vector<int32_t> ri(colptr[nv]);
-        std::vector<double> rx(colptr[nv]);
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j)
-                for (int64_t f = 0; f < nf; ++f) {
-                    const double* g = &m.gb[9 * f];
-                    double v = m.grad_area[f] * einsum_dot3(g + 3 * i, g + 3 * j);
-                    int64_t col = F[3 * f + j];
-                    ri[fill[col]] = F[3 * f + i];
-                    rx[fill[col]] = v;
-                    fill[col]++;
-                }
+        std::vector<int64_t> vptr(nv + 1, 0);
+        for (int64_t q = 0; q < 3 * nf; ++q) vptr[F[q] + 1]++;
+        for (int64_t v = 0; v < nv; ++v) vptr[v + 1] += vptr[v];
+        std::vector<int64_t> vface(3 * nf);
+        {
+            std::vector<int64_t> fill(vptr.begin(), vptr.end() - 1);
+            for (int64_t q = 0; q < 3 * nf; ++q) vface[fill[F[q]]++] = q;  // q = 3 f + corner, ascending f
+        }
+        struct Entry {
+            int32_t row;
+            int64_t pos;
+            double val;
+        };
+        std::vector<Entry> ent;
         m.Lp.assign(nv + 1, 0);
         m.Li.clear(); m.Lx.clear();
-        std::vector<int64_t> idx;
+        m.Li.reserve(7 * nv); m.Lx.reserve(7 * nv);
         for (int64_t c = 0; c < nv; ++c) {
-            idx.resize(colptr[c + 1] - colptr[c]);
-            std::iota(idx.begin(), idx.end(), colptr[c]);
-            std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return ri[a] < ri[b]; });
-            for (size_t k = 0; k < idx.size();) {
+            ent.clear();
+            for (int64_t t = vptr[c]; t < vptr[c + 1]; ++t) {
+                const int64_t f = vface[t] / 3;
+                const int j = (int)(vface[t] - 3 * f);
+                const double* g = &m.gb[9 * f];
+                for (int i = 0; i < 3; ++i)
+                    ent.push_back({F[3 * f + i], (int64_t)(3 * i + j) * nf + f,
+                                   m.grad_area[f] * einsum_dot3(g + 3 * i, g + 3 * j)});
+            }
+            std::sort(ent.begin(), ent.end(),
+                      [](const Entry& a, const Entry& b) { return a.row != b.row ? a.row < b.row : a.pos < b.pos; });
+            for (size_t k = 0; k < ent.size();) {
                 size_t l = k;
-                double s = 0.0;
-                while (l < idx.size() && ri[idx[l]] == ri[idx[k]]) { s += rx[idx[l]]; ++l; }
-                m.Li.push_back(ri[idx[k]]);
-                m.Lx.push_back(s);
+                double sum = 0.0;
+                while (l < ent.size() && ent[l].row == ent[k].row) { sum += ent[l].val; ++l; }
+                m.Li.push_back(ent[k].row);
+                m.Lx.push_back(sum);
                 k = l;
             }
             m.Lp[c + 1] = (int64_t)m.Li.size();
