@@ -291,5 +291,5 @@ def prepare(vertices, faces, cortex_mask) -> PreparedMesh:
         boundary=boundary_vertices(F), health_h=float(np.median(fL)),
         lean_area=np.ascontiguousarray(la), g11=np.ascontiguousarray(g11),
         g12=np.ascontiguousarray(g12), g22=np.ascontiguousarray(g22),
-        bin_width=lean_bin_width(V, F),
+        bin_width=float(np.quantile(fL, 0.999) * 1.05),  # lean_bin_width(V, F): the same edge lengths
     )
