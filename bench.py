@@ -94,9 +94,10 @@ def _cpu_worker(workload, seed, sources, q):
     ho = oracle.HeatOracle(pm.V, pm.F)
     _cpu_source(ho, pm, targets, sources[0])  # warm caches
     t0 = time.perf_counter()
-    for s in sources:
-        _cpu_source(ho, pm, targets, s)
-    q.put((len(sources), time.perf_counter() - t0))
+    recs = [_cpu_source(ho, pm, targets, s) for s in sources]
+    sec = time.perf_counter() - t0
+    keep = ("radii", "perim", "extra_a", "msd_u", "msd_w", "dist_b", "bad")
+    q.put((len(sources), sec, [{k: np.asarray(r[k]).tolist() for k in keep} for r in recs]))
 
 
 def _start_cpu_baseline(workload, seed, n):
@@ -109,7 +110,7 @@ def _start_cpu_baseline(workload, seed, n):
     sources = [int(x) for x in bfs[np.linspace(0, bfs.size - 1, n).astype(int)]]
     p = ctx.Process(target=_cpu_worker, args=(workload, seed, sources, q), daemon=True)
     p.start()
-    return p, q, n
+    return p, q, sources
 
 
 def run_reference(args):
@@ -153,7 +154,7 @@ def run_reference(args):
         "metric": METRIC, "value": value, "unit": "sources/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": _config(args, pm),
+        "config": _config(args, pm, int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": value, "unit": "sources/s", "cores": cores, "kind": "port",
                          "sample": f"{per_step} sources per core per step, BFS-spaced over all "
                                    f"{pm.n_vertices} sources; factorisation ({factor_s:.1f} s) excluded"},
@@ -173,12 +174,37 @@ def _ref_task(srcs):
     return len(srcs)
 
 
-def _config(args, pm):
+def _config(args, pm, world=1):
     return {"workload": f"{args.workload} folded icosphere, {pm.n_vertices} cortical sources, "
                         f"{pm.n_faces} faces, t=(0.7 mm)^2, 12 scales + {N_BETWEEN} samples between",
             "batch_sources_per_step": args.batch, "block_k": args.block_k, "precision": args.precision,
             "pipeline_depth": args.pipeline_depth, "leaf_size": args.leaf_size, "relax": args.relax,
-            "parallelism": f"replicas{args.gpus}", "l2": "inputs larger than L2 (n x K RHS blocks > 126 MB)"}
+            "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (n x K RHS blocks > 126 MB)"}
+
+
+# ---------------------------------------------------------------------------
+# ranks: one process per GPU
+# ---------------------------------------------------------------------------
+def rank_env():
+    """(rank, world size, local rank) of this process, from torchrun's environment."""
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def free_port():
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_ranks(script, argv, nproc, timeout_s=None):
+    """Run `script argv` as nproc processes under torch.distributed.run on this node (rendezvous on
+    127.0.0.1, one rank per GPU); returns the launcher's exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={int(nproc)}",
+           "--master-addr", "127.0.0.1", f"--master-port={free_port()}", script, *argv]
+    return subprocess.call(cmd, timeout=timeout_s)
 
 
 # ---------------------------------------------------------------------------
@@ -269,9 +295,7 @@ def max_over_ranks(x, dist, device):
 
 
 def run_gpu(args):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = rank_env()
     cpu = None
     if rank == 0 and world == 1 and args.cpu_sample > 0:
         cpu = _start_cpu_baseline(args.workload, args.seed, args.cpu_sample)  # before any CUDA call
@@ -357,10 +381,11 @@ def run_gpu(args):
     # CUDA-event span is its own duration, not shared with the other streams ---
     nprof = 3
     K = args.block_k
+    prof_out = torch.empty((K, stride), dtype=torch.float64, device=f"cuda:{dev}")  # a block's records
     eng.profile(True)
     for i in range(nprof):
         j = i % max(1, share.size // K)
-        eng.compute_metrics_device(src_dev[j * K:(j + 1) * K], targets, N_BETWEEN, 1e-6, args.precision, out_dev,
+        eng.compute_metrics_device(src_dev[j * K:(j + 1) * K], targets, N_BETWEEN, 1e-6, args.precision, prof_out,
                                    stream.cuda_stream)
         eng.synchronize(stream.cuda_stream)
     stages, _ = eng.stage_times()
@@ -412,7 +437,7 @@ def run_gpu(args):
             "metric": METRIC, "value": value, "unit": "sources/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 heat / f32 Poisson" if args.precision == "mixed" else "f64",
-            "data": "synthetic", "config": _config(args, pm),
+            "data": "synthetic", "config": _config(args, pm, world),
             "e2e": {"value": e2e, "unit": "sources/s", "h2d_bytes_per_step": B * 4 * world,
                     "d2h_bytes_per_step": B * stride * 8 * world},
             "gpu_launches": launches,
@@ -428,12 +453,13 @@ def run_gpu(args):
         if tuned is not None:
             line["autotune"] = tuned
         if cpu is not None:
-            p, q, n = cpu
+            p, q, cpu_sources = cpu
             try:
-                cnt, sec = q.get(timeout=args.cpu_timeout)
+                cnt, sec, cpu_recs = q.get(timeout=args.cpu_timeout)
                 line["cpu_baseline"] = {"value": cnt / sec, "unit": "sources/s", "cores": 1, "kind": "port",
                                         "sample": f"{cnt} BFS-spaced sources of the same mesh, one at a time, "
                                                   "single thread, factorisation excluded"}
+                line["err_vs_oracle"] = _errors_vs_oracle(eng, cpu_sources, cpu_recs, targets)
             except Exception as exc:
                 line["cpu_baseline"] = {"value": None, "unit": "sources/s", "cores": 1, "kind": "port",
                                         "sample": f"not finished: {exc!r}"}
@@ -443,6 +469,28 @@ def run_gpu(args):
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def _errors_vs_oracle(eng, sources, recs, targets):
+    """Largest relative error of the engine (both forms) against the oracle's FP64 records of the
+    CPU-baseline sample, over the sources neither side flags; and the flag disagreements."""
+    from fastcorticalwiring_b200 import engine as E
+
+    src = np.asarray(sources, dtype=np.int32)
+    obad = np.array([bool(r["bad"]) for r in recs])
+    out = {"sources": int(src.size), "oracle_flagged": int(obad.sum())}
+    for prec in ("fp64", "mixed"):
+        r = E.split_records(eng.compute_metrics(src, targets, N_BETWEEN, precision=prec), 12, N_BETWEEN)
+        ok = ~(obad | r["bad"])
+        e = {"flag_mismatch": int(np.sum(obad != r["bad"]))}
+        for key, okey in (("radii", "radii"), ("perim", "perim"), ("extra_a", "extra_a"), ("msd_u", "msd_u"),
+                          ("msd_w", "msd_w"), ("dist_b", "dist_b")):
+            ref = np.array([np.asarray(x[okey], float) for x in recs])
+            got = np.asarray(r[key], float)
+            rel = np.abs(got[ok] - ref[ok]) / np.maximum(np.abs(ref[ok]), 1e-300)
+            e[key] = float(np.nanmax(rel)) if rel.size else None
+        out[prec] = e
+    return out
 
 
 def _fp64_forms_and_errors(eng, pm, targets, stream, args, dev):
@@ -589,6 +637,14 @@ def main(argv=None):
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    _, world, _ = rank_env()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # one process per GPU: start the ranks here when no launcher did
+        return launch_ranks(os.path.abspath(__file__), sys.argv[1:] if argv is None else list(argv), args.gpus)
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; start one rank per GPU "
+              f"(torchrun --nproc-per-node {args.gpus}) or drop the launcher", file=sys.stderr)
+        return 2
     return run_gpu(args)
 
 

@@ -49,6 +49,21 @@ def classify_nonmanifold_vertices(vertices, faces):
             "also_boundary": non_manifold & boundary, "interior": non_manifold - boundary}
 
 
+def check_interior_nonmanifold(pm, engine_type="b200", allow=False):
+    """Count the cortical submesh's interior non-manifold vertices and warn about them unless
+    allowed, as the reference does for engines without the robust fallback
+    (core_analysis.py:609-636). Returns the count."""
+    n = len(classify_nonmanifold_vertices(pm.V, pm.F)["interior"])
+    if n and not allow:
+        warnings.warn(
+            "Interior non-manifold vertices detected in cortical submesh. "
+            "Automatic use_robust fallback is only available for the potpourri engine; "
+            f"continuing with engine_type={engine_type!r}.",
+            RuntimeWarning,
+        )
+    return n
+
+
 class WiringAnalysis:
     """A cortical mesh, its B200 engine and the per-vertex wiring metrics.
 
@@ -72,15 +87,8 @@ class WiringAnalysis:
         self.allow_interior_nonmanifold = bool(allow_interior_nonmanifold)
         self.mesh = M.prepare(vertices, faces, cortex_mask)
         pm = self.mesh
-        report = classify_nonmanifold_vertices(pm.V, pm.F)
-        self.n_interior_nonmanifold = len(report["interior"])
-        if self.n_interior_nonmanifold and not self.allow_interior_nonmanifold:
-            warnings.warn(
-                "Interior non-manifold vertices detected in cortical submesh. "
-                "Automatic use_robust fallback is only available for the potpourri engine; "
-                f"continuing with engine_type={self.engine_type!r}.",
-                RuntimeWarning,
-            )
+        self.n_interior_nonmanifold = check_interior_nonmanifold(pm, self.engine_type,
+                                                                 self.allow_interior_nonmanifold)
         self.distance_engine = B200DistanceEngine(pm.V, pm.F, **dict(engine_kwargs or {}))
         self.eps = float(eps)
         self.precision = precision

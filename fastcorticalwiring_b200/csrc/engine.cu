@@ -181,6 +181,7 @@ struct fcw_engine {
     std::vector<cudaEvent_t> event_pool;
     double stage_ms[FCW_N_STAGES] = {0};
     int64_t launches = 0;
+    int32_t num_sms = 148;  // the device's multiprocessors (grid sizes of grid-stride kernels)
 
     // Device memory is stream-ordered (the device's default pool): freeing it
     // waits for this engine's streams only, never for other engines' work, so
@@ -353,6 +354,7 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     e->ground_new = (int32_t)(S.n - 1);
 
     FCW_CUDA(cudaSetDevice(e->device));
+    FCW_CUDA(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, e->device));
     FCW_CUDA(fcw::configure_kernels());
     FCW_CUDA(fcw::configure_solve_kernels());
     FCW_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
@@ -1363,8 +1365,10 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
     a.out = out_dev;
     k_map_sources<<<(K + 127) / 128, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)e->sym.n, K, e->cw().src,
                                                    e->err_d);
-    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)e->sym.n, k, K, d_dev, e->iperm_d, e->cw().Y);
+    k_fields_in<<<e->num_sms * 8, 256, 0, st>>>((int32_t)e->sym.n, k, K, d_dev, e->iperm_d, e->cw().Y);
+    mark(e, st, FCW_STAGE_SHIFT);
     fcw::launch_shift_stats<double, double>(a, K, e->cw().Y, e->cw().dT64, st);
+    e->launches += 3;
     metrics_block<double>(e, a, e->cw().dT64, st);
     FCW_CUDA(cudaGetLastError());
     return FCW_OK;
@@ -1468,9 +1472,14 @@ extern "C" int fcw_field_metrics_static(fcw_engine* e, const double* d_dev, cons
     a.near_count = near_count;  // cleared by launch_shift_stats before the shift kernel
     a.out = out_dev;
     k_map_sources<<<1, 128, 0, st>>>(k, sources_dev, e->iperm_d, (int32_t)n, K, src, e->err_d);
-    k_fields_in<<<148 * 8, 256, 0, st>>>((int32_t)n, k, K, d_dev, e->iperm_d, Y);
+    k_fields_in<<<e->num_sms * 8, 256, 0, st>>>((int32_t)n, k, K, d_dev, e->iperm_d, Y);
+    mark(e, st, FCW_STAGE_SHIFT);
     fcw::launch_shift_stats<double, double>(a, K, Y, dT, st);
+    e->launches += 3;
+    mark(e, st, FCW_STAGE_METRICS);
     fcw::launch_source_metrics<double>(a, dT, st);
+    mark(e, st, -1);
+    e->launches += 1;
     FCW_CUDA(cudaGetLastError());
     return FCW_OK;
 }

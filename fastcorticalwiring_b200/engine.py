@@ -98,8 +98,20 @@ class HeatEngine:
         return out
 
     def compute_metrics_device(self, sources_dev, targets, n_between, eps, precision, out_dev, stream) -> None:
-        """Device-resident form: sources_dev/out_dev are torch CUDA tensors (int32 / float64)."""
+        """Device-resident form: sources_dev/out_dev are torch CUDA tensors (int32 / float64).
+
+        out_dev holds one record of metrics_stride(len(targets), n_between) doubles per source."""
         t = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1)
+        import torch
+
+        stride = _lib.metrics_stride(t.size, n_between)
+        if sources_dev.dtype != torch.int32 or not sources_dev.is_contiguous():
+            raise ValueError("sources_dev must be a contiguous int32 tensor")
+        if out_dev.dtype != torch.float64 or not out_dev.is_contiguous():
+            raise ValueError("out_dev must be a contiguous float64 tensor")
+        if out_dev.numel() < sources_dev.numel() * stride:
+            raise ValueError(f"out_dev holds {out_dev.numel()} doubles; {sources_dev.numel()} records of "
+                             f"{stride} need {sources_dev.numel() * stride}")
         _lib.check(_lib.load().fcw_compute_metrics_device(
             self.handle, ctypes.c_void_p(sources_dev.data_ptr()), int(sources_dev.numel()), _precision(precision),
             _lib.ptr(t), t.size, int(n_between), float(eps), ctypes.c_void_p(out_dev.data_ptr()),

@@ -40,11 +40,14 @@ class SubjectAnalysis(A.WiringAnalysis):
     """WiringAnalysis results filled from a serving job's records (no engine of its own)."""
 
     def __init__(self, pm: M.PreparedMesh, engine_info: dict, diffusion_length_mm: float, eps=1e-6,
-                 precision="mixed", metadata=None):
+                 precision="mixed", metadata=None, allow_interior_nonmanifold=False):
         self.mesh = pm
         self.distance_engine = None
         self.engine_type = "b200"
         self.metadata = dict(metadata or {})
+        self.allow_interior_nonmanifold = bool(allow_interior_nonmanifold)
+        self.n_interior_nonmanifold = A.check_interior_nonmanifold(pm, self.engine_type,
+                                                                   self.allow_interior_nonmanifold)
         self._engine_info = dict(engine_info or {})
         self._diffusion_length_mm = float(diffusion_length_mm)
         self.eps = float(eps)

@@ -209,7 +209,10 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
  * FCW_E_INVALID (roughly 34k vertices with 32 fields). It calls no allocator.
  * The first call on each device looks up the array's device address; make that
  * call before any stream capture. Every call reuses the same array, so calls
- * that overlap on the GPU (other streams, other threads) race: serialise them. */
+ * that overlap on the GPU (other streams, other threads) race: serialise them.
+ * Like the other entry points that take a stream, it returns once the work is
+ * enqueued; an invalid source index found on the device is reported by the
+ * next fcw_synchronize on that stream (FCW_E_INVALID). */
 int fcw_field_metrics_static(fcw_engine* e, const double* d_dev, const int32_t* sources_dev, int32_t k,
                              const double* targets_host, int32_t n_targets, int32_t n_between, double eps,
                              double* out_dev, void* stream);

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Generate the golden fixtures from the reference's own code.
 
-Run in a checkout where the FastCorticalWiring reference is importable
-(default /root/reference, or --reference PATH). The tests never run this:
+Run with --reference PATH naming a FastCorticalWiring checkout whose modules
+import (numba, scipy). The tests never run this:
 its outputs are committed next to it as small .npz files.
 
 Reference code run here, unmodified:
@@ -308,7 +308,7 @@ def _geometry_kat(ca, lg, tk):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="folder holding the reference's Python modules")
     ap.add_argument("--only", default=None, help="write only this fixture (file name)")
     args = ap.parse_args()
     sys.path.insert(0, REPO)

@@ -318,10 +318,19 @@ def test_pipelined_blocks_match_single_stream():
     rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
     assert np.all(both_nan | (rel <= 1e-12))
     # the reference method itself flags a few of these fields (corrupted heat fields of the
-    # extrinsic operator); the flags must be the oracle's
+    # extrinsic operator); the flags must be the oracle's, both ways: every engine flag is an
+    # oracle flag and every oracle flag an engine flag (this mixed-precision run may differ
+    # only where the oracle's count sits within two vertices of the threshold)
     import oracle
     r = engine.split_records(a, 12, 3)
     ho = oracle.HeatOracle(pm.V, pm.F)
-    for j in np.flatnonzero(r["bad"]):
-        assert oracle.field_health(ho.distances([src[j]])[0], pm.V, src[j], pm.health_h)[2]
+    phi = ho.distances(src)
+    n = pm.n_vertices
+    borderline = 0
+    for j, s in enumerate(src):
+        neg, viol, bad = oracle.field_health(phi[j], pm.V, s, pm.health_h)
+        if bool(r["bad"][j]) != bad:
+            assert min(abs(neg - 1e-3), abs(viol - 1e-3)) <= 2.0 / n, (j, neg, viol)
+            borderline += 1
+    assert borderline <= 1
     assert np.all(np.isfinite(r["radii"][~r["bad"]]))

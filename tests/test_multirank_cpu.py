@@ -52,3 +52,23 @@ def test_two_ranks_shard_every_source_once_and_time_the_slowest():
         assert np.array_equal(np.concatenate([np.asarray(s) for s in shares]), order)
         assert abs(len(shares[0]) - len(shares[1])) <= 1
     assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
+
+
+def test_launch_ranks_starts_one_process_per_rank(capfd):
+    """bench.launch_ranks (what `bench.py --gpus N` uses when no launcher started it) runs N ranks
+    under torch.distributed.run on 127.0.0.1; here two gloo ranks of a probe script."""
+    probe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "rank_probe.py")
+    rc = bench.launch_ranks(probe, ["1001"], 2, timeout_s=240)
+    assert rc == 0
+    lines = [ln for ln in capfd.readouterr().out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    import json
+
+    got = json.loads(lines[0])
+    assert got["n_gpus"] == 2 and got["parallelism"] == "replicas2"
+    assert sum(got["ranks_sources"]) == 1001 and got["slowest"] == 2.0
+
+
+def test_bench_refuses_a_world_size_that_is_not_gpus(monkeypatch):
+    monkeypatch.setenv("WORLD_SIZE", "3")
+    assert bench.main(["--gpus", "2", "--steps", "1"]) == 2

@@ -90,3 +90,25 @@ def test_subject_analysis_from_records_writes_schema_v3(tmp_path):
     prov = json.loads(str(z["provenance_json"]))
     assert prov["engine"] == "b200" and prov["t_coef"] == 2.0 and prov["n_flagged_fields"] == 1
     assert sa.metadata == {"subject": "s"}
+
+
+def test_subject_analysis_warns_on_interior_nonmanifold_submesh():
+    """Batch subjects get the same interior non-manifold warning as a single-subject analysis
+    (core_analysis.py:628-635), and the count is kept on the subject."""
+    from fastcorticalwiring_b200 import mesh as M
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    mesh = folded_icosphere(3, seed=1)
+    V, F = mesh.vertices, mesh.faces
+    a, b = F[0, 0], F[0, 1]
+    V2 = np.vstack([V, V[a] + 1.0])
+    F2 = np.vstack([F, [a, b, len(V)], [b, a, len(V)]])
+    pm = M.prepare(V2, F2, np.ones(len(V2), bool))
+    with pytest.warns(RuntimeWarning, match="Interior non-manifold vertices"):
+        sa = runner.SubjectAnalysis(pm, {}, 0.7)
+    assert sa.n_interior_nonmanifold == 2
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        quiet = runner.SubjectAnalysis(pm, {}, 0.7, allow_interior_nonmanifold=True)
+    assert quiet.n_interior_nonmanifold == 2

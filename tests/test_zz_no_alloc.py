@@ -53,3 +53,53 @@ def test_static_entry_matches_allocating_entry_on_consecutive_calls():
         assert ei.value.code == _lib.FCW_E_INVALID and "at most 32 fields" in str(ei.value)
     finally:
         eng.close()
+
+
+def test_static_entry_first_on_a_fresh_engine_matches_the_reference_and_allocates_nothing():
+    """Called first on a fresh engine (no allocating metrics call before it), the static entry
+    point reproduces the reference's own geometry on the reference's fields; a repeated call
+    leaves both the device's free memory and the engine's device-byte count unchanged; and a
+    source index outside the mesh is reported by the next fcw_synchronize, as for the other
+    stream entry points."""
+    import torch
+
+    z = dict(np.load(os.path.join(GOLDEN, "golden_heat_L4.npz")))
+    pm = M.prepare(z["V"], z["F"], z["mask"])
+    eng = engine.HeatEngine(pm.V, pm.F)
+    lib = _lib.load()
+    try:
+        t = np.ascontiguousarray(z["targets"], dtype=np.float64)
+        stride = _lib.metrics_stride(t.size, 3)
+        d = torch.tensor(np.ascontiguousarray(z["phi"]), dtype=torch.float64, device="cuda")
+        src = torch.tensor(z["sources_sub"], dtype=torch.int32, device="cuda")
+        out = torch.full((src.numel(), stride), float("nan"), dtype=torch.float64, device="cuda")
+
+        def run(sources=src):
+            _lib.check(lib.fcw_field_metrics_static(eng.handle, d.data_ptr(), sources.data_ptr(), sources.numel(),
+                                                    _lib.ptr(t), t.size, 3, 1e-6, out.data_ptr(), None))
+            eng.synchronize(0)
+            return out.cpu().numpy()
+
+        bytes0 = eng.info()["device_bytes"]
+        r = engine.split_records(run(), t.size, 3)
+        assert not r["bad"].any()
+        for key in ("radii", "perim", "extra_r", "extra_a"):
+            rel = np.abs(r[key] - z[key]) / np.maximum(np.abs(z[key]), 1e-300)
+            assert np.max(rel) <= 1e-12, (key, np.max(rel))
+        assert np.array_equal(np.float32(r["dist_b"]), z["f32_dist_to_boundary"])
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        run()
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0
+        assert eng.info()["device_bytes"] == bytes0
+        bad = torch.tensor([0, pm.n_vertices + 5], dtype=torch.int32, device="cuda")
+        with pytest.raises(_lib.FCWError) as ei:
+            run(bad)
+        assert ei.value.code == _lib.FCW_E_INVALID and "source index" in str(ei.value)
+        # the error word is cleared once reported: the next call succeeds
+        r2 = engine.split_records(run(), t.size, 3)
+        assert np.array_equal(r2["radii"], r["radii"])
+    finally:
+        eng.close()
