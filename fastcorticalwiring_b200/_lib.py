@@ -26,7 +26,7 @@ EXPORTED = (
     "fcw_compute_distances", "fcw_compute_metrics", "fcw_compute_metrics_device", "fcw_synchronize",
     "fcw_heat_solve_device", "fcw_divergence_device", "fcw_poisson_solve_device", "fcw_field_metrics_device",
     "fcw_engine_profile", "fcw_engine_graphs", "fcw_engine_stage_times", "fcw_field_metrics_static",
-    "fcw_samples_capacity", "fcw_assemble_samples_device", "fcw_assemble_samples",
+    "fcw_samples_capacity", "fcw_assemble_samples_device", "fcw_assemble_samples", "fcw_tc_product_check",
 )
 STAGES = ("heat_fwd", "heat_bwd", "divergence", "poisson_fwd", "poisson_bwd", "shift", "metrics")
 
@@ -42,6 +42,7 @@ class FCWParams(ctypes.Structure):
         ("build_mixed", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("pipeline_depth", ctypes.c_int32),
+        ("tc_sweeps", ctypes.c_int32),
     ]
 
 
@@ -108,6 +109,7 @@ def load():
         "fcw_samples_capacity": (ctypes.c_int, [I32, I32]),
         "fcw_assemble_samples_device": (ctypes.c_int, [P, I64, I32, I32, P, D, P, P, P, P]),
         "fcw_assemble_samples": (ctypes.c_int, [P, P, I64, I32, I32, P, D, P, P, P]),
+        "fcw_tc_product_check": (ctypes.c_int, [P, P, P, I32, I32, I32, I32, I32, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -153,6 +153,11 @@ struct fcw_engine {
     int64_t n_urows = 0, n_parts = 0;
     double *val_h = nullptr, *inv_h = nullptr, *val_p = nullptr, *inv_p = nullptr;
     float *val_g = nullptr, *inv_g = nullptr;
+    // tensor-core FP32 sweeps: core arrays of the grounded factor and the forward task list
+    float *core_hi = nullptr, *core_lo = nullptr;
+    int64_t* core_ptr_d = nullptr;
+    int2* tc_fwd_tasks = nullptr;
+    std::vector<int32_t> tc_fwd_ptr;
     fcw::FaceData fd;
     int32_t* iperm_d = nullptr;
     int32_t* perm_d = nullptr;
@@ -254,7 +259,9 @@ int check_kernel_errors(fcw_engine* e, const char* where) {
         if (h & fcw::KERR_HIST_OVERFLOW) what += " too many distance bins for one source;";
         if (h & fcw::KERR_SCRATCH) what += " per-source face list overflow;";
         if (h & fcw::KERR_ARGS) what += " invalid source index or launch arguments;";
-        return fail((h & fcw::KERR_ARGS) ? FCW_E_INVALID : FCW_E_NUMERIC, std::string(where) + ":" + what);
+        if (h & fcw::KERR_TIMEOUT) what += " a bounded device wait expired;";
+        const int code = (h & fcw::KERR_ARGS) ? FCW_E_INVALID : (h & fcw::KERR_TIMEOUT) ? FCW_E_TIMEOUT : FCW_E_NUMERIC;
+        return fail(code, std::string(where) + ":" + what);
     }
     return FCW_OK;
 }
@@ -303,6 +310,7 @@ int validate_params(const fcw_params* p) {
         return fail(FCW_E_INVALID, "max_width must be in [1, 64] and leaf_size >= 1");
     if (p->relax < 1 || p->relax > p->max_width) return fail(FCW_E_INVALID, "relax must be in [1, max_width]");
     if (p->pipeline_depth < 1 || p->pipeline_depth > 8) return fail(FCW_E_INVALID, "pipeline_depth must be in [1, 8]");
+    if (p->tc_sweeps != 0 && p->tc_sweeps != 1) return fail(FCW_E_INVALID, "tc_sweeps must be 0 or 1");
     return FCW_OK;
 }
 
@@ -357,6 +365,7 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     FCW_CUDA(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, e->device));
     FCW_CUDA(fcw::configure_kernels());
     FCW_CUDA(fcw::configure_solve_kernels());
+    FCW_CUDA(fcw::configure_tc_kernels());
     FCW_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     FCW_CUDA(cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming));
     e->pool.resize((size_t)std::max(1, e->prm.pipeline_depth));
@@ -424,7 +433,8 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
         }
         e->n_urows = uoff[NS];
         e->n_parts = parts;
-        std::vector<int2> ft, bt;
+        std::vector<int2> ft, bt, tft;
+        e->tc_fwd_ptr.assign(S.nlevels + 1, 0);
         e->fwd_ptr.assign(S.nlevels + 1, 0);
         e->bwd_ptr.assign(S.nlevels + 1, 0);
         e->level_rows.assign(S.nlevels, fcw::kMaxWidth);
@@ -448,6 +458,13 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
             }
             e->fwd_ptr[l + 1] = (int32_t)ft.size();
             e->bwd_ptr[l + 1] = (int32_t)bt.size();
+            // tensor-core forward: per supernode the inverse block's product, then 64-row update chunks
+            for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
+                const int32_t s = S.level_nodes[q];
+                const int32_t ns = S.sn_c0[s + 1] - S.sn_c0[s], nr = S.sn_m[s] - ns;
+                for (int32_t c = 0; c <= (nr + 63) / 64; ++c) tft.push_back(make_int2(s, c));
+            }
+            e->tc_fwd_ptr[l + 1] = (int32_t)tft.size();
         }
         const int64_t nfront = S.sn_rowptr[NS];
         std::vector<int32_t> gptr(nfront + 1, 0), gsrc(e->n_urows), gchild(e->n_urows);
@@ -473,6 +490,7 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
         if (e->n_urows > INT32_MAX || nfront > INT32_MAX) return fail(FCW_E_INVALID, "mesh too large for 32-bit update indices");
         FCW_TRY(e->upload(&e->fwd_tasks, ft));
         FCW_TRY(e->upload(&e->bwd_tasks, bt));
+        FCW_TRY(e->upload(&e->tc_fwd_tasks, tft));
         FCW_TRY(e->upload(&e->uoff_d, uoff));
         FCW_TRY(e->upload(&e->poff_d, poff));
         FCW_TRY(e->upload(&e->nsplit_d, nsplit));
@@ -612,6 +630,19 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
         FCW_TRY(e->dalloc(&e->inv_g, S.n_inv));
         fcw::launch_to_float(S.nnz_factor, val_tmp, e->val_g, e->stream);
         fcw::launch_to_float(S.n_inv, inv_tmp, e->inv_g, e->stream);
+        if (e->prm.tc_sweeps) {
+            std::vector<int64_t> cptr(S.nsuper + 1, 0);
+            for (int32_t s = 0; s < S.nsuper; ++s) {
+                const int64_t ns = S.sn_c0[s + 1] - S.sn_c0[s], nr = S.sn_m[s] - ns;
+                const int64_t ns8 = (ns + 7) / 8 * 8, nr32 = (nr + 31) / 32 * 32;
+                cptr[s + 1] = cptr[s] + ns8 * (ns8 + nr32);
+            }
+            FCW_TRY(e->upload(&e->core_ptr_d, cptr));
+            FCW_TRY(e->dalloc(&e->core_hi, (size_t)cptr[S.nsuper]));
+            FCW_TRY(e->dalloc(&e->core_lo, (size_t)cptr[S.nsuper]));
+            fcw::launch_build_cores(e->plan, val_tmp, inv_tmp, e->core_ptr_d, e->core_hi, e->core_lo, e->stream);
+            FCW_CUDA(cudaGetLastError());
+        }
         FCW_CUDA(cudaStreamSynchronize(e->stream));
         e->release(val_tmp);
         e->release(inv_tmp);
@@ -709,6 +740,10 @@ fcw::SolveArgs<T> solve_args(fcw_engine* e, const T* val, const T* inv, T* B, in
     a.part = reinterpret_cast<T*>(e->cw().part);
     a.counters = e->cw().counters;
     a.ktiles = e->cw().K / fcw::kRhsTile;
+    a.core_hi = e->core_hi;
+    a.core_lo = e->core_lo;
+    a.core_ptr = e->core_ptr_d;
+    a.err = e->err_d;
     return a;
 }
 
@@ -741,17 +776,39 @@ void heat_solve(fcw_engine* e, int32_t K, cudaStream_t st) {
     sweep<double>(e, a, st, FCW_STAGE_HEAT_FWD, FCW_STAGE_HEAT_BWD);
 }
 
+// FP32 sweeps on the tensor cores: the same level schedule, the forward with its own task list.
+int sweep_tc(fcw_engine* e, fcw::SolveArgs<float> a, cudaStream_t st) {
+    const auto& S = e->sym;
+    CUtensorMap rmap, bmap;
+    if (fcw::make_rows_map(&rmap, a.R, S.n, a.K) || fcw::make_rows_map(&bmap, a.B, S.n, a.K))
+        return fail(FCW_E_CUDA, "cuTensorMapEncodeTiled failed for the Poisson right-hand sides");
+    mark(e, st, FCW_STAGE_POISSON_FWD);
+    a.tasks = e->tc_fwd_tasks;
+    for (int32_t l = 0; l < S.nlevels; ++l)
+        fcw::launch_fwd_level_tc(a, e->tc_fwd_ptr[l], e->tc_fwd_ptr[l + 1] - e->tc_fwd_ptr[l], rmap, st);
+    mark(e, st, FCW_STAGE_POISSON_BWD);
+    a.tasks = e->bwd_tasks;
+    for (int32_t l = S.nlevels - 1; l >= 0; --l)
+        fcw::launch_bwd_level_tc(a, e->bwd_ptr[l], e->bwd_ptr[l + 1] - e->bwd_ptr[l], bmap, st);
+    e->launches += 2 * (int64_t)S.nlevels;
+    return FCW_OK;
+}
+
 // Poisson solve: right-hand sides R, solution into Y (both n x K, elimination order).
 template <typename T>
-void poisson_solve(fcw_engine* e, const T* val, const T* inv, const T* R, T* Y, int32_t K, cudaStream_t st) {
+int poisson_solve(fcw_engine* e, const T* val, const T* inv, const T* R, T* Y, int32_t K, cudaStream_t st) {
     fcw::SolveArgs<T> a = solve_args<T>(e, val, inv, Y, K);
     a.R = R;
+    if constexpr (sizeof(T) == 4) {
+        if (e->core_hi && K % fcw::kTcCols == 0) return sweep_tc(e, a, st);
+    }
     sweep<T>(e, a, st, FCW_STAGE_POISSON_FWD, FCW_STAGE_POISSON_BWD);
+    return FCW_OK;
 }
 
 // Distances for the K sources in ws.src, shifted, source-major in ws.dT64 / ws.dT32.
 // With metric arguments, the shift also produces the health/MSD partials and near lists.
-void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, const fcw::MetricArgs* ma = nullptr) {
+int distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, const fcw::MetricArgs* ma = nullptr) {
     Workspace& w = e->cw();
     const int32_t n = (int32_t)e->sym.n;
     heat_solve(e, K, st);
@@ -759,18 +816,19 @@ void distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, c
     if (precision == FCW_PREC_MIXED) {
         float* Y = reinterpret_cast<float*>(w.Y);
         fcw::launch_divergence_mixed(e->fd, w.Bh, w.Bp32, K, e->ground_new, st);
-        poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, Y, K, st);
+        FCW_TRY(poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, Y, K, st));
         mark(e, st, FCW_STAGE_SHIFT);
         if (ma) fcw::launch_shift_stats<float, float>(*ma, K, Y, w.dT32, st);
         else fcw::launch_shift_transpose<float, float>(n, K, Y, w.src, w.dT32, st);
     } else {
         fcw::launch_divergence_fp64(e->fd, w.Bh, w.Bp64, K, st);
-        poisson_solve<double>(e, e->val_p, e->inv_p, w.Bp64, w.Y, K, st);
+        FCW_TRY(poisson_solve<double>(e, e->val_p, e->inv_p, w.Bp64, w.Y, K, st));
         mark(e, st, FCW_STAGE_SHIFT);
         if (ma) fcw::launch_shift_stats<double, double>(*ma, K, w.Y, w.dT64, st);
         else fcw::launch_shift_transpose<double, double>(n, K, w.Y, w.src, w.dT64, st);
     }
     e->launches += 2;
+    return FCW_OK;
 }
 
 int metric_args(fcw_engine* e, const double* targets, int32_t nt, int32_t nb, double eps, int32_t nsrc,
@@ -885,6 +943,7 @@ void fcw_default_params(fcw_params* p) {
     p->build_mixed = 1;
     p->device = 0;
     p->pipeline_depth = 4;
+    p->tc_sweeps = 1;
 }
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between) {
@@ -1032,7 +1091,7 @@ int fcw_compute_distances(fcw_engine* e, const int32_t* sources, int64_t n, int3
         const int32_t K = round_k(nb);
         FCW_TRY(ensure_workspace(e, K, e->cw().out_stride));
         FCW_TRY(map_sources_host(e, sources + b0, nb, K, e->stream, buf));
-        distances_block(e, K, precision, e->stream);
+        FCW_TRY(distances_block(e, K, precision, e->stream));
         FCW_CUDA(cudaGetLastError());
         for (int64_t r = 0; r < nb; ++r) {
             if (precision == FCW_PREC_MIXED) {
@@ -1063,20 +1122,20 @@ namespace {
 // captured once per workspace and set of arguments, and replayed for later blocks.
 int block_chain(fcw_engine* e, Workspace& w, int32_t K, int32_t precision, fcw::MetricArgs& a,
                 const double* targets, int32_t nt, int32_t nb, double eps) {
-    auto launch = [&]() {
+    auto launch = [&]() -> int {
         k_map_block_sources<<<(K + 127) / 128, 128, 0, w.stream>>>(w.desc, e->iperm_d, (int32_t)e->sym.n, K, w.src,
                                                                    e->err_d);
         e->launches += 1;
-        distances_block(e, K, precision, w.stream, &a);
+        const int rc = distances_block(e, K, precision, w.stream, &a);
+        if (rc != FCW_OK) return rc;
         if (precision == FCW_PREC_MIXED) metrics_block<float>(e, a, w.dT32, w.stream);
         else metrics_block<double>(e, a, w.dT64, w.stream);
+        return FCW_OK;
     };
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     FCW_CUDA(cudaStreamIsCapturing(w.stream, &cs));
-    if (!e->graphs_on || e->prof_on || cs != cudaStreamCaptureStatusNone) {  // (inside a caller's capture: join it)
-        launch();
-        return FCW_OK;
-    }
+    if (!e->graphs_on || e->prof_on || cs != cudaStreamCaptureStatusNone)  // (inside a caller's capture: join it)
+        return launch();
     std::vector<double> key = {(double)K, (double)precision, (double)nt, (double)nb, eps};
     key.insert(key.end(), targets, targets + nt);
     Workspace::Graph* hit = nullptr;
@@ -1090,10 +1149,15 @@ int block_chain(fcw_engine* e, Workspace& w, int32_t K, int32_t precision, fcw::
         }
         const int64_t l0 = e->launches;
         FCW_CUDA(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal));
-        launch();
+        const int lrc = launch();
         cudaGraph_t g = nullptr;
         cudaGraphExec_t exec = nullptr;
         cudaError_t ce = cudaStreamEndCapture(w.stream, &g);
+        if (lrc != FCW_OK) {
+            if (g) cudaGraphDestroy(g);
+            e->launches = l0;
+            return lrc;
+        }
         if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, g, 0);
         if (g) cudaGraphDestroy(g);
         const int64_t captured = e->launches - l0;  // kernels in the chain (counted when it runs)
@@ -1101,8 +1165,7 @@ int block_chain(fcw_engine* e, Workspace& w, int32_t K, int32_t precision, fcw::
         if (ce != cudaSuccess) {  // not capturable here: launch directly from now on
             cudaGetLastError();
             e->graphs_on = false;
-            launch();
-            return FCW_OK;
+            return launch();
         }
         w.graphs.push_back({key, exec, captured});
         hit = &w.graphs.back();
@@ -1341,7 +1404,7 @@ int fcw_poisson_solve_device(fcw_engine* e, const double* div_dev, const int32_t
                                                    e->err_d);
     FCW_CUDA(cudaMemsetAsync(e->cw().Bp64, 0, (size_t)e->sym.n * K * sizeof(double), st));
     fcw::launch_permute_rows((int32_t)e->sym.n, k, div_dev, k, nullptr, e->cw().Bp64, K, e->iperm_d, st);
-    poisson_solve<double>(e, e->val_p, e->inv_p, e->cw().Bp64, e->cw().Y, K, st);
+    FCW_TRY(poisson_solve<double>(e, e->val_p, e->inv_p, e->cw().Bp64, e->cw().Y, K, st));
     fcw::launch_shift_transpose<double, double>((int32_t)e->sym.n, K, e->cw().Y, e->cw().src, e->cw().dT64, st);
     // phi_dev[old][c] = dT[c][iperm[old]]: transpose back through the permute kernel, column by column
     for (int32_t c = 0; c < k; ++c)

@@ -1,6 +1,7 @@
 // Device kernels of the heat-method pipeline and their host launchers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -12,6 +13,7 @@ enum : int {
     KERR_HIST_OVERFLOW = 2,   // more distance bins than the geometry kernel holds
     KERR_SCRATCH = 4,         // per-source face list overflow
     KERR_ARGS = 8,            // inconsistent launch arguments
+    KERR_TIMEOUT = 16,        // a bounded wait (mbarrier, tensor-core completion) expired
 };
 
 constexpr int kMaxWidth = 64;      // widest supernode the dense kernels accept
@@ -81,6 +83,13 @@ struct SolveArgs {
     int* counters = nullptr;             // per (supernode, column tile) arrival tickets, zero at rest
     int32_t ktiles = 0;                  // column tiles the counters were sized for
     int32_t stage = 0;                   // forward: children's update rows staged per chunk (set by the launcher)
+    // FP32 tensor-core sweeps: per supernode the stacked [inv(L_ss); Q_s] split into TF32 hi and
+    // lo terms, in core-matrix order (tc.cuh), ns8 = round_up(ns, 8) columns and ns8 +
+    // round_up(nr, 32) rows (padding zero)
+    const float* core_hi = nullptr;
+    const float* core_lo = nullptr;
+    const int64_t* core_ptr = nullptr;   // per supernode: offset (floats) of its core array
+    int* err = nullptr;                  // error bits (bounded waits that expired)
 };
 
 cudaError_t configure_solve_kernels();
@@ -94,6 +103,23 @@ void launch_fwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, bool ga
 template <typename T>
 void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, int32_t tile_rows, cudaStream_t st);
 void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st);
+
+// FP32 sweeps on the tensor cores (tcgen05.mma kind::tf32, each operand split into two TF32
+// terms, three products accumulated in tensor memory); K a multiple of 64, 64 columns per CTA.
+// Forward tasks are (supernode, c): c = 0 forms X_s = inv(L_ss) W, c >= 1 the update rows
+// [64 (c - 1), 64 c). Backward tasks are those of launch_bwd_level. rows_map is a tiled tensor
+// map of the sweep's own-row input (forward: R, backward: B) made by make_rows_map.
+constexpr int kTcCols = 64;
+void launch_fwd_level_tc(const SolveArgs<float>& a, int32_t t0, int32_t ntasks, const CUtensorMap& rows_map,
+                         cudaStream_t st);
+void launch_bwd_level_tc(const SolveArgs<float>& a, int32_t t0, int32_t ntasks, const CUtensorMap& rows_map,
+                         cudaStream_t st);
+cudaError_t configure_tc_kernels();
+// Tensor map of an n x K row-major FP32 array: boxes of 64 rows x 32 columns, 128-byte swizzle.
+int make_rows_map(CUtensorMap* map, const float* base, int64_t n, int32_t K);
+// The core arrays of the tensor-core sweeps from the FP64 panels and inverse blocks.
+void launch_build_cores(const DevPlan& p, const double* val, const double* inv, const int64_t* core_ptr,
+                        float* hi, float* lo, cudaStream_t st);
 
 // ---- fused gradient -> normalise -> divergence (face.cu) ----
 struct FaceData {

@@ -1,0 +1,163 @@
+// Blackwell (sm_100a) primitives for the FP32 sweeps: tcgen05 tensor-core
+// products with TMEM accumulators, TMA bulk copies completing on mbarriers,
+// and the split of FP32 operands into two TF32 terms.
+//
+// Operand layouts are the "no swizzle" canonical layouts of the UMMA shared
+// memory descriptor. The unit is a core matrix of 128 contiguous bytes:
+// 8 rows of 16 bytes (4 FP32/TF32 values).
+//   * K-major (A = M x K, K contiguous): core (m/8, k/4) holds rows m%8, each
+//     with 4 consecutive k. LBO = byte stride between k-chunks of 4, SBO =
+//     byte stride between groups of 8 rows.
+//   * MN-major (B = K x N, N contiguous): core (k/8, n/4) holds 8 k-rows, each
+//     with 4 consecutive n. LBO = byte stride between groups of 8 k, SBO =
+//     byte stride between n-chunks of 4.
+// Both place element (outer8, inner4) of a core matrix at byte
+// (outer8 % 8) * 16 + (inner4 % 4) * 4, so one array of cores serves as a
+// K-major A and, read with LBO and SBO swapped, as the MN-major transpose.
+#pragma once
+
+#include <cuda.h>
+#include <stdint.h>
+
+namespace fcw {
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// FP32 -> TF32, round to nearest (ties away from zero); the result is an FP32 value
+// whose 13 low mantissa bits are zero, so the tensor core reads it exactly.
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+// x = hi + lo + O(2^-22 |x|): hi and lo both TF32 (x - hi is exact in FP32).
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+    hi = to_tf32(x);
+    lo = to_tf32(x - hi);
+}
+
+// Byte offset of element (outer, inner) in a core-matrix array whose cores are
+// ordered outer-group major: core (outer/8, inner/4) at index (outer/8) * icores + inner/4.
+__host__ __device__ __forceinline__ uint32_t core_offset(int outer, int inner, int icores) {
+    return (uint32_t)((((outer >> 3) * icores + (inner >> 2)) << 7) + ((outer & 7) << 4) + ((inner & 3) << 2));
+}
+
+// UMMA shared-memory descriptor, no swizzle, version 1 (sm_100).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// Instruction descriptor of tcgen05.mma kind::tf32 with an FP32 accumulator.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool a_mn_major, bool b_mn_major, bool negate_a) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((negate_a ? 1u : 0u) << 13) | ((a_mn_major ? 1u : 0u) << 15) |
+           ((b_mn_major ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A * B, one thread issues.
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+// Arrive on mbar once every tcgen05.mma this thread issued before has completed.
+__device__ __forceinline__ void mma_commit(uint64_t* mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Generic-proxy writes to shared memory become visible to the tensor core / TMA.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// ---- tensor memory (one full warp allocates and frees) ----
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+                 "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// 32 lanes x 16 consecutive columns: thread i of the warp gets lane (taddr.lane + i).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---- mbarriers ----
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the phase with this parity to complete, for at most about limit_ns
+// nanoseconds; false if it did not.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit_ns = 2000000000ull) {
+    if (mbar_try_wait(b, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (;;) {
+        for (int i = 0; i < 64; ++i)
+            if (mbar_try_wait(b, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+}
+
+// ---- TMA (unicast, this GPU's memory only) ----
+// Contiguous bytes global -> shared; the mbarrier's transaction count drops by `bytes`
+// when they land. Addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(sdst)),
+        "l"(gsrc), "r"(bytes), "r"(smem_u32(mbar))
+        : "memory");
+}
+// A 2D box of a tiled tensor map (coordinates: x innermost, in elements).
+__device__ __forceinline__ void tma_load_2d(void* sdst, const CUtensorMap* map, int x, int y, uint64_t* mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(sdst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(mbar))
+        : "memory");
+}
+
+}  // namespace tc
+}  // namespace fcw

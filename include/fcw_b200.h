@@ -49,6 +49,7 @@ typedef struct fcw_params {
     int32_t build_mixed;        /* also factor the grounded FP32 Poisson operator */
     int32_t device;             /* CUDA device ordinal */
     int32_t pipeline_depth;     /* blocks in flight on separate streams in the device metrics path (1-8) */
+    int32_t tc_sweeps;          /* mixed Poisson sweeps on the tensor cores (1, default) or FMA tiles (0) */
 } fcw_params;
 
 typedef struct fcw_info {
@@ -92,7 +93,8 @@ enum {
     FCW_N_STAGES = 7
 };
 
-/* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 64, mixed on, 4 blocks in flight). */
+/* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 64, mixed on, 4 blocks in flight,
+ * tensor-core Poisson sweeps). */
 void fcw_default_params(fcw_params* p);
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between);
@@ -198,6 +200,17 @@ int fcw_poisson_solve_device(fcw_engine* e, const double* div_dev, const int32_t
 int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* sources_dev, int32_t k,
                              const double* targets_host, int32_t n_targets, int32_t n_between, double eps,
                              double* out_dev, void* stream);
+
+/* One tensor-core product tile of the mixed Poisson sweeps, for checking their
+ * arithmetic (no reference counterpart): C = A B (trans = 0, A m x k row-major)
+ * or C = P^T B (trans = 1, P k x m row-major), B k x n row-major, C m x n, all
+ * FP32 device arrays; m <= 128, k <= 64, n in {64, 128}. Each operand is split into
+ * two TF32 terms and terms = 3 accumulates hi*hi + hi*lo + lo*hi (terms = 1: hi*hi)
+ * with tcgen05.mma in tensor memory, through the sweeps' shared-memory layouts.
+ * raw_dev (nullable) receives the 128 x n accumulator lanes; status_dev (one int,
+ * zero on entry) gets a nonzero bit if the completion wait expired. */
+int fcw_tc_product_check(const float* a_dev, const float* b_dev, float* c_dev, int32_t m, int32_t k, int32_t n,
+                         int32_t terms, int32_t trans, float* raw_dev, int32_t* status_dev, void* stream);
 
 /* Allocation-free field metrics, for callers that may not allocate device
  * memory while they run: a host that reserves the device for its own memory
