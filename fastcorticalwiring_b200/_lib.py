@@ -27,6 +27,7 @@ EXPORTED = (
     "fcw_heat_solve_device", "fcw_divergence_device", "fcw_poisson_solve_device", "fcw_field_metrics_device",
     "fcw_engine_profile", "fcw_engine_graphs", "fcw_engine_stage_times", "fcw_field_metrics_static",
     "fcw_samples_capacity", "fcw_assemble_samples_device", "fcw_assemble_samples", "fcw_tc_product_check",
+    "fcw_intrinsic_operators",
 )
 STAGES = ("heat_fwd", "heat_bwd", "divergence", "poisson_fwd", "poisson_bwd", "shift", "metrics")
 
@@ -43,6 +44,7 @@ class FCWParams(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("pipeline_depth", ctypes.c_int32),
         ("tc_sweeps", ctypes.c_int32),
+        ("robust", ctypes.c_int32),
     ]
 
 
@@ -57,6 +59,7 @@ class FCWInfo(ctypes.Structure):
         ("analyze_ms", ctypes.c_double), ("factor_ms", ctypes.c_double), ("flops_factor", ctypes.c_double),
         ("device_bytes", ctypes.c_int64),
         ("pipeline_depth", ctypes.c_int32), ("block_k", ctypes.c_int32),
+        ("n_flips", ctypes.c_int64),
     ]
 
     def as_dict(self):
@@ -110,6 +113,7 @@ def load():
         "fcw_assemble_samples_device": (ctypes.c_int, [P, I64, I32, I32, P, D, P, P, P, P]),
         "fcw_assemble_samples": (ctypes.c_int, [P, P, I64, I32, I32, P, D, P, P, P]),
         "fcw_tc_product_check": (ctypes.c_int, [P, P, P, I32, I32, I32, I32, I32, P, P, P]),
+        "fcw_intrinsic_operators": (ctypes.c_int, [P, I64, P, I64, P, P, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -171,3 +175,30 @@ def mesh_arrays(V, F):
     bf = np.empty(nv, dtype=np.uint8)
     check(load().fcw_mesh_arrays(ptr(V), nv, ptr(F), nf, ptr(va), ptr(la), ptr(g11), ptr(g12), ptr(g22), ptr(bf)))
     return dict(vertex_area=va, lean_area=la, g11=g11, g12=g12, g22=g22, boundary=np.flatnonzero(bf).astype(np.int32))
+
+
+def intrinsic_operators(V, F):
+    """The robust operators on the host: dict with nflips, L (scipy CSC), mass, and the
+    flipped tufted cover (tri, len, twin over 2 n_faces faces; None when nothing flipped)."""
+    import scipy.sparse as sp
+
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    F = np.ascontiguousarray(F, dtype=np.int32)
+    nv, nf = V.shape[0], F.shape[0]
+    nfl, nnz = ctypes.c_int64(0), ctypes.c_int64(0)
+    lib = load()
+    check(lib.fcw_intrinsic_operators(ptr(V), nv, ptr(F), nf, ctypes.byref(nfl), ctypes.byref(nnz),
+                                      None, None, None, None, None, None, None))
+    Lp = np.empty(nv + 1, np.int64)
+    Li = np.empty(nnz.value, np.int32)
+    Lx = np.empty(nnz.value, np.float64)
+    mass = np.empty(nv, np.float64)
+    tri = np.empty(6 * nf, np.int32)
+    ln = np.empty(6 * nf, np.float64)
+    tw = np.empty(6 * nf, np.int32)
+    check(lib.fcw_intrinsic_operators(ptr(V), nv, ptr(F), nf, ctypes.byref(nfl), ctypes.byref(nnz), ptr(Lp),
+                                      ptr(Li), ptr(Lx), ptr(mass), ptr(tri), ptr(ln), ptr(tw)))
+    flipped = nfl.value > 0
+    return dict(nflips=int(nfl.value), L=sp.csc_matrix((Lx, Li, Lp), shape=(nv, nv)), mass=mass,
+                tri=tri.reshape(2 * nf, 3) if flipped else None, len=ln.reshape(2 * nf, 3) if flipped else None,
+                twin=tw.reshape(2 * nf, 3) if flipped else None)

@@ -40,6 +40,10 @@ int fail(int code, const std::string& msg) {
         if (rc_ != FCW_OK) return rc_; \
     } while (0)
 
+// Triangle-inequality margin of the robust operators' mollified edge lengths, relative to
+// the mean edge length (the default of Sharp & Crane's intrinsic mollification).
+constexpr double kMollifyFactor = 1e-6;
+
 double now_ms() {
     using namespace std::chrono;
     return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
@@ -187,6 +191,7 @@ struct fcw_engine {
     double stage_ms[FCW_N_STAGES] = {0};
     int64_t launches = 0;
     int32_t num_sms = 148;  // the device's multiprocessors (grid sizes of grid-stride kernels)
+    int64_t n_flips = 0;    // intrinsic edge flips of the robust operators
 
     // Device memory is stream-ordered (the device's default pool): freeing it
     // waits for this engine's streams only, never for other engines' work, so
@@ -311,6 +316,7 @@ int validate_params(const fcw_params* p) {
     if (p->relax < 1 || p->relax > p->max_width) return fail(FCW_E_INVALID, "relax must be in [1, max_width]");
     if (p->pipeline_depth < 1 || p->pipeline_depth > 8) return fail(FCW_E_INVALID, "pipeline_depth must be in [1, 8]");
     if (p->tc_sweeps != 0 && p->tc_sweeps != 1) return fail(FCW_E_INVALID, "tc_sweeps must be 0 or 1");
+    if (p->robust != 0 && p->robust != 1) return fail(FCW_E_INVALID, "robust must be 0 or 1");
     return FCW_OK;
 }
 
@@ -352,6 +358,8 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     std::string err;
     double t0 = now_ms();
     if (fcw::prepare_mesh(V, nv, F, nf, e->mesh, err)) return fail(FCW_E_INVALID, err);
+    if (e->prm.robust && fcw::intrinsic_delaunay(e->mesh, kMollifyFactor, e->n_flips, err))
+        return fail(FCW_E_INVALID, err);
     e->t_coef = std::pow(e->prm.diffusion_length_mm / e->mesh.mean_edge, 2.0);
     e->t = e->t_coef * e->mesh.mean_edge * e->mesh.mean_edge;
     if (fcw::build_symbolic(e->mesh, e->prm.leaf_size, e->prm.max_width, e->prm.relax, e->sym, err)) return fail(FCW_E_INVALID, err);
@@ -944,6 +952,7 @@ void fcw_default_params(fcw_params* p) {
     p->device = 0;
     p->pipeline_depth = 4;
     p->tc_sweeps = 1;
+    p->robust = 0;
 }
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between) {
@@ -987,6 +996,8 @@ int fcw_analyze(const double* V, int64_t nv, const int32_t* F, int64_t nf, const
     std::string err;
     double t0 = now_ms();
     if (fcw::prepare_mesh(V, nv, F, nf, m, err)) return fail(FCW_E_INVALID, err);
+    int64_t nflips = 0;
+    if (params->robust && fcw::intrinsic_delaunay(m, kMollifyFactor, nflips, err)) return fail(FCW_E_INVALID, err);
     if (fcw::build_symbolic(m, params->leaf_size, params->max_width, params->relax, S, err)) return fail(FCW_E_INVALID, err);
     if (info) {
         std::memset(info, 0, sizeof(*info));
@@ -1007,8 +1018,32 @@ int fcw_analyze(const double* V, int64_t nv, const int32_t* F, int64_t nf, const
         info->total_vertex_area = m.total_area;
         info->analyze_ms = now_ms() - t0;
         info->flops_factor = S.flops_factor;
+        info->n_flips = nflips;
     }
     if (perm_out) std::memcpy(perm_out, S.perm.data(), nv * sizeof(int32_t));
+    return FCW_OK;
+}
+
+int fcw_intrinsic_operators(const double* V, int64_t nv, const int32_t* F, int64_t nf, int64_t* nflips, int64_t* nnz,
+                            int64_t* Lp, int32_t* Li, double* Lx, double* mass, int32_t* tri, double* len,
+                            int32_t* twin) {
+    if (!V || !F) return fail(FCW_E_INVALID, "vertices/faces is NULL");
+    fcw::MeshPrep m;
+    std::string err;
+    if (fcw::prepare_mesh(V, nv, F, nf, m, err)) return fail(FCW_E_INVALID, err);
+    int64_t nfl = 0;
+    if (fcw::intrinsic_delaunay(m, kMollifyFactor, nfl, err)) return fail(FCW_E_INVALID, err);
+    if (nflips) *nflips = nfl;
+    if (nnz) *nnz = (int64_t)m.Li.size();
+    if (Lp) std::memcpy(Lp, m.Lp.data(), (nv + 1) * sizeof(int64_t));
+    if (Li) std::memcpy(Li, m.Li.data(), m.Li.size() * sizeof(int32_t));
+    if (Lx) std::memcpy(Lx, m.Lx.data(), m.Lx.size() * sizeof(double));
+    if (mass) std::memcpy(mass, m.mass.data(), nv * sizeof(double));
+    if (nfl > 0) {
+        if (tri) std::memcpy(tri, m.itri.data(), m.itri.size() * sizeof(int32_t));
+        if (len) std::memcpy(len, m.ilen.data(), m.ilen.size() * sizeof(double));
+        if (twin) std::memcpy(twin, m.itwin.data(), m.itwin.size() * sizeof(int32_t));
+    }
     return FCW_OK;
 }
 
@@ -1066,6 +1101,7 @@ int fcw_engine_info(const fcw_engine* e, fcw_info* info) {
     info->device_bytes = e->bytes;
     info->pipeline_depth = (int32_t)e->pool.size();
     info->block_k = e->prm.block_k;
+    info->n_flips = e->n_flips;
     return FCW_OK;
 }
 

@@ -29,9 +29,18 @@ struct MeshPrep {
     std::vector<int64_t> Lp;
     std::vector<int32_t> Li;
     std::vector<double> Lx;
+    // after intrinsic_delaunay flipped some edge: the intrinsic triangulation (corner
+    // vertices per face, length and twin per halfedge, -1 on fixed edges)
+    std::vector<int32_t> itri, itwin;
+    std::vector<double> ilen;
 };
 
 int prepare_mesh(const double* V, int64_t nv, const int32_t* F, int64_t nf, MeshPrep& out, std::string& err);
+
+// Replace L and the lumped mass by those of the intrinsic Delaunay triangulation
+// (intrinsic.cpp); mollify_factor scales the mean edge length into the triangle
+// inequality margin. nflips = 0 leaves the operators untouched.
+int intrinsic_delaunay(MeshPrep& m, double mollify_factor, int64_t& nflips, std::string& err);
 
 // ---------------------------------------------------------------------------
 // Symbolic sparse Cholesky analysis (host). All indices are in the

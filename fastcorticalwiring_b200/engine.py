@@ -28,7 +28,7 @@ MIN_DIFFUSION_LENGTH_MM = 0.5              # distance_engines.py:13
 RECOMMENDED_MIN_DIFFUSION_LENGTH_MM = 0.7  # distance_engines.py:14
 
 ENGINE_DEFAULTS = dict(block_k=1024, leaf_size=64, max_width=64, relax=64, build_mixed=1, device=0, pipeline_depth=4,
-                       tc_sweeps=1)
+                       tc_sweeps=1, robust=0)
 
 
 class HeatEngine:
@@ -226,27 +226,28 @@ class BaseDistanceEngine(ABC):
 
 
 class B200DistanceEngine(BaseDistanceEngine):
-    """Heat-method distances on a B200, one source per call (FP64, consistent operators).
+    """Heat-method distances on a B200, one source per call (FP64).
 
     Keyword rules follow PotpourriDistanceEngine (distance_engines.py:75-125):
     `diffusion_length_mm` (default 0.7) must be finite and >= 0.5 (ValueError),
     values below 0.7 warn (RuntimeWarning); `t_coef` is rejected.
     `allow_eigen_fallback` is accepted and ignored (there is no SuiteSparse
-    backend to check). The engine has no intrinsic-Delaunay ("robust")
-    operators, so `use_robust=True` raises instead of being silently ignored. Other keys are engine tunables (block_k,
-    leaf_size, max_width, relax, build_mixed, device, pipeline_depth).
+    backend to check). Other keys are engine tunables (block_k, leaf_size,
+    max_width, relax, build_mixed, device, pipeline_depth, tc_sweeps).
 
-    The operators are the extrinsic cotan Laplacian L = G^T diag(A) G and the
-    barycentric lumped mass (fastcw_lean.py:394-413), so `use_robust` is False.
+    `use_robust` picks the operators. False (the default): the consistent
+    extrinsic cotan Laplacian L = G^T diag(A) G and barycentric lumped mass of
+    fastcw_lean.py:394-413, the method the engine is checked against. True: the
+    cotan Laplacian and lumped mass of the intrinsic Delaunay triangulation, as
+    the production potpourri3d engine uses (distance_engines.py:119-125); the
+    normalised gradient and its divergence stay on the mesh's faces.
     """
 
     def __init__(self, vertices, faces, **engine_kwargs):
         super().__init__(vertices, faces, **engine_kwargs)
         kw = dict(self.engine_kwargs)
         kw.pop("allow_eigen_fallback", None)
-        if "use_robust" in kw and bool(kw.pop("use_robust")):
-            raise ValueError("use_robust=True is not supported by the b200 engine; it uses the extrinsic "
-                             "cotan operators (use_robust=False).")
+        robust = bool(kw.pop("use_robust", False))
         if "t_coef" in kw:
             raise ValueError("Set diffusion_length_mm instead of t_coef.")
         L = float(kw.pop("diffusion_length_mm", DEFAULT_DIFFUSION_LENGTH_MM))
@@ -255,12 +256,14 @@ class B200DistanceEngine(BaseDistanceEngine):
         if L < RECOMMENDED_MIN_DIFFUSION_LENGTH_MM:
             warnings.warn(f"diffusion_length_mm={L} is below the validated {RECOMMENDED_MIN_DIFFUSION_LENGTH_MM} mm.",
                           RuntimeWarning)
-        unknown = set(kw) - set(ENGINE_DEFAULTS) - {"poisson_shift"}
+        unknown = set(kw) - set(ENGINE_DEFAULTS) - {"poisson_shift"} - {"robust"}
         if unknown:
             raise ValueError(f"Unsupported engine kwargs for b200 engine: {', '.join(sorted(unknown))}")
+        kw["robust"] = int(robust)
         self._engine = HeatEngine(self.vertices, self.faces, diffusion_length_mm=L, **kw)
         info = self._engine.info()
-        self.use_robust = False
+        self.use_robust = robust
+        self.n_flips = int(info["n_flips"])
         self.diffusion_length_mm = L
         self.mean_edge_length = float(info["mean_edge_length"])
         self.t_coef = float(info["t_coef"])

@@ -50,6 +50,9 @@ typedef struct fcw_params {
     int32_t device;             /* CUDA device ordinal */
     int32_t pipeline_depth;     /* blocks in flight on separate streams in the device metrics path (1-8) */
     int32_t tc_sweeps;          /* mixed Poisson sweeps on the tensor cores (1, default) or FMA tiles (0) */
+    int32_t robust;             /* 1: operators of the intrinsic Delaunay triangulation (use_robust,
+                                   distance_engines.py:119-125); 0 (default): the extrinsic cotan
+                                   operators of fastcw_lean.py:394-413 */
 } fcw_params;
 
 typedef struct fcw_info {
@@ -66,6 +69,7 @@ typedef struct fcw_info {
     int64_t device_bytes;       /* device memory held by the engine */
     int32_t pipeline_depth;     /* blocks in flight the device holds workspaces for (<= params) */
     int32_t block_k;            /* sources per block */
+    int64_t n_flips;            /* intrinsic edge flips (robust operators; 0 otherwise) */
 } fcw_info;
 
 /* Per-source metric record: FCW_M_* offsets, then radii[nt], perimeters[nt],
@@ -113,6 +117,19 @@ int fcw_analyze(const double* vertices, int64_t n_vertices, const int32_t* faces
 int fcw_mesh_arrays(const double* vertices, int64_t n_vertices, const int32_t* faces, int64_t n_faces,
                     double* vertex_area, double* lean_area, double* g11, double* g12, double* g22,
                     uint8_t* boundary_flag);
+
+/* The robust operators on the host (no device): the intrinsic Delaunay
+ * triangulation by edge flips and its cotan Laplacian and lumped mass, as the
+ * engine builds them when params->robust is set. First call with Lp == NULL to
+ * get *nflips and *nnz; then Lp (n_vertices + 1), Li and Lx (nnz) receive L as
+ * full symmetric CSC, mass (n_vertices) the lumped mass, and, when nflips > 0, the
+ * flipped tufted cover (2 n_faces faces: the mesh's faces, then their back sides):
+ * tri (3 corner vertices per cover face), len and twin (one per halfedge h =
+ * 3 face + corner, from corner to the next; twin -1 on non-manifold edges). Any
+ * output pointer may be NULL. */
+int fcw_intrinsic_operators(const double* vertices, int64_t n_vertices, const int32_t* faces, int64_t n_faces,
+                            int64_t* nflips, int64_t* nnz, int64_t* Lp, int32_t* Li, double* Lx, double* mass,
+                            int32_t* tri, double* len, int32_t* twin);
 
 /* Build the engine: operators, symbolic analysis, device factorisation of
  * M + tL and L + shift*M (and the grounded FP32 Poisson operator when

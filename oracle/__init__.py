@@ -22,6 +22,7 @@ from .heat import (  # noqa: F401
     field_eval,
     source_metrics,
 )
+from .intrinsic import intrinsic_delaunay, robust_operators  # noqa: F401
 from .samples import (  # noqa: F401
     boundary_area_loss_fraction,
     clean_vertex_samples,

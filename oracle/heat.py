@@ -8,7 +8,9 @@ reference code they restate:
 * operators               fastcw_lean.py:394-413
 * normalized_divergence   fastcw_lean.py:416-442   (C, lean_oracle.c)
 * HeatOracle              fastcw_lean.py:467-531   (factor of M + tL and L + shift*M,
-                                                    delta RHS, shift phi(s) = 0)
+                                                    delta RHS, shift phi(s) = 0); robust=True
+                                                    takes L and M from oracle.intrinsic
+                                                    (distance_engines.py:119-125)
 * field_health            lean_geometry.py:343-357
 * msd_and_boundary        core_analysis.py:1566-1581
 * source_geometry         lean_geometry.py:302-340 (C, lean_oracle.c)
@@ -197,10 +199,16 @@ class HeatOracle:
     Poisson operator L + shift * M (fastcw_lean.py:500).
     """
 
-    def __init__(self, V, F, diffusion_length_mm=0.7, poisson_shift=1e-10, t_coef=None, ordering="dissection"):
+    def __init__(self, V, F, diffusion_length_mm=0.7, poisson_shift=1e-10, t_coef=None, ordering="dissection",
+                 robust=False):
         V = np.ascontiguousarray(V, dtype=np.float64)
         F = np.ascontiguousarray(F, dtype=np.int32)
         L, mass, area, g0, g1, g2 = operators(V, F)
+        self.n_flips = 0
+        if robust:  # intrinsic Delaunay L and M; the divergence stays on the mesh's faces
+            from .intrinsic import robust_operators
+
+            L, mass, self.n_flips = robust_operators(V, F)
         h = mean_edge_length(V, F)
         if t_coef is None:
             t_coef = (float(diffusion_length_mm) / h) ** 2

@@ -85,7 +85,7 @@ def test_symbolic_structure_contains_true_fill(level):
 
 def test_engine_kwarg_rules_follow_potpourri_engine():
     z, pm = _l4()
-    for bad in ({"use_robust": True}, {"t_coef": 1.0}, {"diffusion_length_mm": 0.4},
+    for bad in ({"t_coef": 1.0}, {"diffusion_length_mm": 0.4},
                 {"diffusion_length_mm": float("nan")}, {"not_a_setting": 1}):
         with pytest.raises(ValueError):
             engine.B200DistanceEngine(pm.V, pm.F, **bad)
