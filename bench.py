@@ -328,7 +328,7 @@ def run_gpu(args):
                  "trials": [{k: (round(v, 1) if isinstance(v, float) else v) for k, v in t.items()} for t in trials]}
     t0 = time.perf_counter()
     eng = E.HeatEngine(pm.V, pm.F, device=dev, block_k=args.block_k, pipeline_depth=args.pipeline_depth,
-                       leaf_size=args.leaf_size, relax=args.relax)
+                       leaf_size=args.leaf_size, relax=args.relax, tc_sweeps=int(args.tc_sweeps))
     eng.graphs(not args.no_graphs)
     build_s = time.perf_counter() - t0
     info = eng.info()
@@ -446,7 +446,8 @@ def run_gpu(args):
             "clocks": clk,
             "engine": {"factor_ms": info["factor_ms"], "analyze_ms": info["analyze_ms"], "build_s": build_s,
                        "n_supernodes": info["n_supernodes"], "n_levels": info["n_levels"],
-                       "nnz_factor": info["nnz_factor"], "device_bytes": info["device_bytes"],
+                       "nnz_factor": info["nnz_factor"], "nnz_l": info["nnz_l"],
+                       "device_bytes": info["device_bytes"], "tc_sweeps": bool(args.tc_sweeps),
                        "pipeline_depth_held": info["pipeline_depth"], "cuda_graphs": not args.no_graphs},
         }
         line.update(extra)
@@ -625,6 +626,8 @@ def main(argv=None):
     ap.add_argument("--ref-sources-per-core", type=int, default=2)
     ap.add_argument("--quick", action="store_true", help="skip the FP64 forms and the accuracy check")
     ap.add_argument("--no-graphs", action="store_true", help="launch each block's kernels directly")
+    ap.add_argument("--tc-sweeps", type=int, default=1, choices=(0, 1),
+                    help="mixed Poisson sweeps on the tensor cores (1) or on FMA register tiles (0)")
     ap.add_argument("--autotune", action="store_true", help="choose block size and depth on the mesh first")
     ap.add_argument("--serving", action="store_true", help="run the serving stream instead (own JSON line)")
     ap.add_argument("--serving-jobs", type=int, default=64)

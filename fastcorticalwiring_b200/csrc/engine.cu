@@ -83,6 +83,17 @@ __global__ void k_map_block_sources(const fcw::BlockDesc* __restrict__ d, const 
     out[k] = v;
 }
 
+// Rows [0, k) of dT (K x n, one field per source, elimination order) -> out (k x n, caller order).
+template <typename T>
+__global__ void k_fields_out(int32_t n, int32_t k, const T* __restrict__ dT, const int32_t* __restrict__ iperm,
+                             double* __restrict__ out) {
+    const int64_t total = (int64_t)k * n;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / n), i = (int)(e - (int64_t)r * n);
+        out[e] = (double)dT[(int64_t)r * n + iperm[i]];
+    }
+}
+
 // d (k rows, caller vertex order) -> Y (n x K vertex-major, elimination order); columns >= k are zero.
 __global__ void k_fields_in(int32_t n, int32_t k, int32_t K, const double* __restrict__ d,
                             const int32_t* __restrict__ iperm, double* __restrict__ Y) {
@@ -182,6 +193,8 @@ struct fcw_engine {
     float *hsr_d = nullptr, *hsa_d = nullptr;  // staging for the host-buffer sample assembly
     int32_t* hcnt_d = nullptr;
     int64_t hcap_smp = 0, hcap_cnt = 0;
+    double* hdist_d = nullptr;  // staging for the host-buffer distances API (caller order)
+    int64_t hcap_dist = 0;
     double analyze_ms = 0.0, factor_ms = 0.0;
     double lean_total = 0.0;  // sum of the lean face areas (the prefix total of a finite field)
     // stage timeline (CUDA events on the working stream), off unless enabled
@@ -466,11 +479,13 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
             }
             e->fwd_ptr[l + 1] = (int32_t)ft.size();
             e->bwd_ptr[l + 1] = (int32_t)bt.size();
-            // tensor-core forward: per supernode the inverse block's product, then 64-row update chunks
+            // tensor-core forward: per supernode the inverse block with the first 64 update rows,
+            // then 128-row update chunks
             for (int32_t q = S.level_ptr[l]; q < S.level_ptr[l + 1]; ++q) {
                 const int32_t s = S.level_nodes[q];
                 const int32_t ns = S.sn_c0[s + 1] - S.sn_c0[s], nr = S.sn_m[s] - ns;
-                for (int32_t c = 0; c <= (nr + 63) / 64; ++c) tft.push_back(make_int2(s, c));
+                const int32_t nchunk = 1 + std::max(0, (nr - 64 + 127) / 128);
+                for (int32_t c = 0; c < nchunk; ++c) tft.push_back(make_int2(s, c));
             }
             e->tc_fwd_ptr[l + 1] = (int32_t)tft.size();
         }
@@ -935,6 +950,55 @@ int32_t round_k(int64_t k) { return (int32_t)(((k + fcw::kRhsTile - 1) / fcw::kR
 
 }  // namespace
 
+namespace {
+
+// Run `launch` (a chain of launches on w.stream) captured as a CUDA graph, once per
+// workspace and key, and replayed after that; directly while graphs are off, the stage
+// timeline is on, or the stream is already being captured by the caller.
+template <class F>
+int run_chain(fcw_engine* e, Workspace& w, const std::vector<double>& key, F&& launch) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    FCW_CUDA(cudaStreamIsCapturing(w.stream, &cs));
+    if (!e->graphs_on || e->prof_on || cs != cudaStreamCaptureStatusNone) return launch();
+    Workspace::Graph* hit = nullptr;
+    for (auto& g : w.graphs)
+        if (g.key == key) hit = &g;
+    if (!hit) {
+        constexpr size_t kMaxGraphs = 4;  // e.g. a full block and a call's last, partial one
+        if (w.graphs.size() >= kMaxGraphs) {
+            cudaGraphExecDestroy(w.graphs.front().exec);
+            w.graphs.erase(w.graphs.begin());
+        }
+        const int64_t l0 = e->launches;
+        FCW_CUDA(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal));
+        const int lrc = launch();
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(w.stream, &g);
+        if (lrc != FCW_OK) {
+            if (g) cudaGraphDestroy(g);
+            e->launches = l0;
+            return lrc;
+        }
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        const int64_t captured = e->launches - l0;  // kernels in the chain (counted when it runs)
+        e->launches = l0;
+        if (ce != cudaSuccess) {  // not capturable here: launch directly from now on
+            cudaGetLastError();
+            e->graphs_on = false;
+            return launch();
+        }
+        w.graphs.push_back({key, exec, captured});
+        hit = &w.graphs.back();
+    }
+    FCW_CUDA(cudaGraphLaunch(hit->exec, w.stream));
+    e->launches += hit->launches;
+    return FCW_OK;
+}
+
+}  // namespace
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -1120,28 +1184,34 @@ int fcw_compute_distances(fcw_engine* e, const int32_t* sources, int64_t n, int3
     const int32_t Kmax = e->prm.block_k;
     const int64_t nv = e->sym.n;
     std::vector<int32_t> buf;
-    std::vector<double> rowbuf(nv);
-    std::vector<float> rowbuf32(nv);
     for (int64_t b0 = 0; b0 < n; b0 += Kmax) {
         const int64_t nb = std::min<int64_t>(Kmax, n - b0);
         const int32_t K = round_k(nb);
         FCW_TRY(ensure_workspace(e, K, e->cw().out_stride));
-        FCW_TRY(map_sources_host(e, sources + b0, nb, K, e->stream, buf));
-        FCW_TRY(distances_block(e, K, precision, e->stream));
-        FCW_CUDA(cudaGetLastError());
-        for (int64_t r = 0; r < nb; ++r) {
-            if (precision == FCW_PREC_MIXED) {
-                FCW_CUDA(cudaMemcpyAsync(rowbuf32.data(), e->cw().dT32 + r * nv, nv * sizeof(float),
-                                         cudaMemcpyDeviceToHost, e->stream));
-                FCW_CUDA(cudaStreamSynchronize(e->stream));
-                for (int64_t i = 0; i < nv; ++i) out_host[(b0 + r) * nv + i] = (double)rowbuf32[e->sym.iperm[i]];
-            } else {
-                FCW_CUDA(cudaMemcpyAsync(rowbuf.data(), e->cw().dT64 + r * nv, nv * sizeof(double),
-                                         cudaMemcpyDeviceToHost, e->stream));
-                FCW_CUDA(cudaStreamSynchronize(e->stream));
-                for (int64_t i = 0; i < nv; ++i) out_host[(b0 + r) * nv + i] = rowbuf[e->sym.iperm[i]];
-            }
+        if (e->hcap_dist < nb * nv) {
+            if (e->hdist_d) e->release(e->hdist_d);
+            e->hdist_d = nullptr;
+            FCW_TRY(e->dalloc(&e->hdist_d, (size_t)(nb * nv)));
+            e->hcap_dist = nb * nv;
         }
+        Workspace& w = e->cw();
+        FCW_TRY(map_sources_host(e, sources + b0, nb, K, w.stream, buf));
+        // the chain (solves, divergence, shift, fields back to the caller's order) as one graph
+        const std::vector<double> key = {(double)K, (double)precision, -1.0, (double)nb};
+        FCW_TRY(run_chain(e, w, key, [&]() -> int {
+            FCW_TRY(distances_block(e, K, precision, w.stream));
+            const int grid = e->num_sms * 8;
+            if (precision == FCW_PREC_MIXED)
+                k_fields_out<float><<<grid, 256, 0, w.stream>>>((int32_t)nv, (int32_t)nb, w.dT32, e->iperm_d, e->hdist_d);
+            else
+                k_fields_out<double><<<grid, 256, 0, w.stream>>>((int32_t)nv, (int32_t)nb, w.dT64, e->iperm_d, e->hdist_d);
+            e->launches += 1;
+            return FCW_OK;
+        }));
+        FCW_CUDA(cudaGetLastError());
+        FCW_CUDA(cudaMemcpyAsync(out_host + b0 * nv, e->hdist_d, (size_t)(nb * nv) * sizeof(double),
+                                 cudaMemcpyDeviceToHost, w.stream));
+        FCW_CUDA(cudaStreamSynchronize(w.stream));
         FCW_TRY(check_kernel_errors(e, "distances"));
     }
     return FCW_OK;
@@ -1168,47 +1238,9 @@ int block_chain(fcw_engine* e, Workspace& w, int32_t K, int32_t precision, fcw::
         else metrics_block<double>(e, a, w.dT64, w.stream);
         return FCW_OK;
     };
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    FCW_CUDA(cudaStreamIsCapturing(w.stream, &cs));
-    if (!e->graphs_on || e->prof_on || cs != cudaStreamCaptureStatusNone)  // (inside a caller's capture: join it)
-        return launch();
     std::vector<double> key = {(double)K, (double)precision, (double)nt, (double)nb, eps};
     key.insert(key.end(), targets, targets + nt);
-    Workspace::Graph* hit = nullptr;
-    for (auto& g : w.graphs)
-        if (g.key == key) hit = &g;
-    if (!hit) {
-        constexpr size_t kMaxGraphs = 4;  // e.g. a full block and a call's last, partial one
-        if (w.graphs.size() >= kMaxGraphs) {
-            cudaGraphExecDestroy(w.graphs.front().exec);
-            w.graphs.erase(w.graphs.begin());
-        }
-        const int64_t l0 = e->launches;
-        FCW_CUDA(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal));
-        const int lrc = launch();
-        cudaGraph_t g = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(w.stream, &g);
-        if (lrc != FCW_OK) {
-            if (g) cudaGraphDestroy(g);
-            e->launches = l0;
-            return lrc;
-        }
-        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, g, 0);
-        if (g) cudaGraphDestroy(g);
-        const int64_t captured = e->launches - l0;  // kernels in the chain (counted when it runs)
-        e->launches = l0;
-        if (ce != cudaSuccess) {  // not capturable here: launch directly from now on
-            cudaGetLastError();
-            e->graphs_on = false;
-            return launch();
-        }
-        w.graphs.push_back({key, exec, captured});
-        hit = &w.graphs.back();
-    }
-    FCW_CUDA(cudaGraphLaunch(hit->exec, w.stream));
-    e->launches += hit->launches;
-    return FCW_OK;
+    return run_chain(e, w, key, launch);
 }
 
 }  // namespace

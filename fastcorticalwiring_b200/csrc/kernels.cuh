@@ -106,8 +106,8 @@ void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reac
 
 // FP32 sweeps on the tensor cores (tcgen05.mma kind::tf32, each operand split into two TF32
 // terms, three products accumulated in tensor memory); K a multiple of 64, 64 columns per CTA.
-// Forward tasks are (supernode, c): c = 0 forms X_s = inv(L_ss) W, c >= 1 the update rows
-// [64 (c - 1), 64 c). Backward tasks are those of launch_bwd_level. rows_map is a tiled tensor
+// Forward tasks are (supernode, c): c = 0 forms X_s = inv(L_ss) W and update rows [0, 64),
+// c >= 1 update rows [64 + 128 (c - 1), 64 + 128 c). Backward tasks are those of launch_bwd_level. rows_map is a tiled tensor
 // map of the sweep's own-row input (forward: R, backward: B) made by make_rows_map.
 constexpr int kTcCols = 64;
 void launch_fwd_level_tc(const SolveArgs<float>& a, int32_t t0, int32_t ntasks, const CUtensorMap& rows_map,

@@ -22,7 +22,7 @@
 //     mbarrier, and the accumulator comes back through tcgen05.ld to a shared
 //     tile that is written out with 16-byte row-segment stores.
 //
-// A CTA is one task x 64 columns (the MMA's N); M = 64. Every wait (TMA and
+// A CTA is one task x 64 columns (the MMA's N); M = 128 forward, 64 backward. Every wait (TMA and
 // MMA completion) is bounded: past about two seconds the CTA raises
 // KERR_TIMEOUT in a.err, frees its tensor memory and returns.
 #include "kernels.cuh"
@@ -35,7 +35,8 @@ namespace {
 constexpr int TCN = kTcCols;            // right-hand-side columns per CTA (N of the MMA)
 constexpr int TCM = 64;                 // rows of a task's product (M of the MMA)
 constexpr int TC_LS = TCN + 4;          // row stride (floats) of the output and gathered-row tiles
-constexpr int TC_STAGE = 64;            // children's update rows staged per gather chunk
+constexpr int TC_STAGE = 48;            // children's update rows staged per gather chunk (forward)
+constexpr int TCF = 128;                // rows of a forward task's product (M = 128)
 constexpr int TC_RC = 32;               // structure rows per backward chunk
 constexpr int TC_PT = kMaxWidth;        // rows of a backward partial-sum slot
 constexpr uint32_t TC_TILE = 64u * TCN * 4u;   // a 64 x 64 FP32 tile (16 KB)
@@ -142,14 +143,15 @@ __device__ __forceinline__ void split_gathered(const float* Xg, int nk, float* B
     }
 }
 
-// D (+)= A B over ksteps steps of K = 8 with two TF32 terms per operand. A is K-major
+// D (+)= A B (M rows) over ksteps steps of K = 8 with two TF32 terms per operand. A is K-major
 // (a_mn = false: 8-row groups a_sbo apart, k-chunks 128 bytes apart, 256 bytes per step)
 // or MN-major (a_mn = true: the transposed read of a core array, 4-column chunks 128 bytes
 // apart, k-groups a_lbo apart, one group per step). B is MN-major with 16 n-chunks.
+template <int M>
 __device__ __forceinline__ void issue_split_mma(uint32_t d, const float* Ahi, const float* Alo, uint32_t a_cores,
                                                 bool a_mn, const float* Bhi, const float* Blo, int ksteps,
                                                 bool accumulate) {
-    const uint32_t idesc = tc::idesc_tf32(TCM, TCN, a_mn, true, false);
+    const uint32_t idesc = tc::idesc_tf32(M, TCN, a_mn, true, false);
     const uint32_t ah = tc::smem_u32(Ahi), al = tc::smem_u32(Alo), bh = tc::smem_u32(Bhi), bl = tc::smem_u32(Blo);
     const uint32_t a_lbo = a_mn ? a_cores * 128u : 128u, a_sbo = a_mn ? 128u : a_cores * 128u;
     const uint32_t a_step = a_mn ? a_cores * 128u : 256u;
@@ -194,24 +196,31 @@ __device__ __forceinline__ unsigned char* align1k(unsigned char* p) {
 }
 
 // ---------------------------------------------------------------------------
-// Forward: task (s, c), c = 0: X_s = inv(L_ss) W; c >= 1: U_s rows [64(c-1), 64c) = Q W + children.
-// Shared memory: R0 = A hi | A lo (32 KB; the output tile after the product), R1 = own-row
+// Forward: task (s, c) is one M = 128 product with W (the supernode's right-hand side less
+// its children's update rows). c = 0: rows [0, 64) of A are inv(L_ss) (X_s, written to B)
+// and rows [64, 128) the first 64 rows of Q_s (update rows [0, 64)); c >= 1: 128 rows of
+// Q_s, update rows [64 + 128 (c - 1), ...). Update rows get the children's rows that land
+// on them and go to U for the parent.
+// Shared memory: R0 = A hi | A lo (64 KB; the output tile after the product), R1 = own-row
 // TMA tile, then B hi | B lo (32 KB), R2 = children's update rows (TC_STAGE x 64 floats).
 // ---------------------------------------------------------------------------
-constexpr size_t kFwdTcSmem = 1024 + 4 * TC_TILE + (size_t)TC_STAGE * TCN * 4;
+constexpr uint32_t TC_FTILE = (uint32_t)TCF * 64u * 4u;  // one A term: 128 rows x 64 columns (32 KB)
+constexpr size_t kFwdTcSmem = 1024 + 2 * (size_t)TC_FTILE + 2 * TC_TILE + (size_t)TC_STAGE * TCN * 4;
+
+__device__ __forceinline__ int fwd_first_row(int chunk) { return chunk == 0 ? 0 : 64 + (chunk - 1) * TCF; }
 
 __global__ void __launch_bounds__(NT, 2) k_fwd_tc(SolveArgs<float> a, int32_t t0, int32_t ntiles,
                                                  const __grid_constant__ CUtensorMap rmap) {
     extern __shared__ unsigned char smraw_tc[];
     unsigned char* sm = align1k(smraw_tc);
     float* Ahi = reinterpret_cast<float*>(sm);
-    float* Alo = reinterpret_cast<float*>(sm + TC_TILE);
+    float* Alo = reinterpret_cast<float*>(sm + TC_FTILE);
     float* Ot = reinterpret_cast<float*>(sm);
-    unsigned char* Tt = sm + 2 * TC_TILE;
-    float* Bhi = reinterpret_cast<float*>(sm + 2 * TC_TILE);
-    float* Blo = reinterpret_cast<float*>(sm + 3 * TC_TILE);
-    float* St = reinterpret_cast<float*>(sm + 4 * TC_TILE);
-    __shared__ int grs[TCM + 1];
+    unsigned char* Tt = sm + 2 * TC_FTILE;
+    float* Bhi = reinterpret_cast<float*>(sm + 2 * TC_FTILE);
+    float* Blo = reinterpret_cast<float*>(sm + 2 * TC_FTILE + TC_TILE);
+    float* St = reinterpret_cast<float*>(sm + 2 * TC_FTILE + 2 * TC_TILE);
+    __shared__ int grs[TCF + 1];
     __shared__ unsigned char live[TC_STAGE];
     __shared__ uint64_t bar_ld, bar_mma;
     __shared__ uint32_t tbase;
@@ -221,18 +230,18 @@ __global__ void __launch_bounds__(NT, 2) k_fwd_tc(SolveArgs<float> a, int32_t t0
     const int2 task = a.tasks[t0 + ti];
     const int s = task.x, chunk = task.y;
     const DevPlan& p = a.p;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int K = a.K, k0 = tile * TCN;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, nr = p.sn_m[s] - ns;
     const int ns8 = (ns + 7) & ~7, nr32 = (nr + 31) & ~31;
     const int64_t fb = p.sn_rowptr[s];
     const bool xtask = chunk == 0;
-    const int q0 = xtask ? 0 : (chunk - 1) * TCM;
-    const int nq = xtask ? ns : min(TCM, nr - q0);
-    const int arow0 = xtask ? 0 : ns8 + q0;
-    const int arows = xtask ? ns8 : min(TCM, nr32 - q0);
-    const uint32_t abytes = (uint32_t)arows * (uint32_t)ns8 * 4u;
-    const int64_t aoff = a.core_ptr[s] + (int64_t)arow0 * ns8;
+    const int q0 = fwd_first_row(chunk);             // first update row of the task
+    const int qrows = xtask ? 64 : TCF;               // update rows the task's product holds
+    const int nq = max(0, min(qrows, nr - q0));       // of which real
+    const int qa = max(0, min(qrows, nr32 - q0));     // Q rows in the core array (padding zero)
+    const uint32_t row_bytes = (uint32_t)ns8 * 4u;
+    const int64_t cbase = a.core_ptr[s];
 
     if (tid == 0) {
         tc::mbar_init(&bar_ld, 1);
@@ -246,15 +255,26 @@ __global__ void __launch_bounds__(NT, 2) k_fwd_tc(SolveArgs<float> a, int32_t t0
     tc::fence_after_sync();
     const uint32_t tmem = tbase;
     if (tid == 0) {
-        tc::mbar_arrive_expect_tx(&bar_ld, 2 * abytes + TC_TILE);
-        tc::bulk_load(Ahi, a.core_hi + aoff, abytes, &bar_ld);
-        tc::bulk_load(Alo, a.core_lo + aoff, abytes, &bar_ld);
+        // A rows: [0, ns8) the inverse (chunk 0), then from row 64 (chunk 0) or 0 the Q rows
+        const uint32_t inv_bytes = xtask ? (uint32_t)ns8 * row_bytes : 0u;
+        const uint32_t q_bytes = (uint32_t)qa * row_bytes;
+        const uint32_t qdst = (xtask ? 64u : 0u) * (uint32_t)(ns8 >> 2) * 16u;  // 8-row groups of ns8/4 cores
+        tc::mbar_arrive_expect_tx(&bar_ld, 2 * (inv_bytes + q_bytes) + TC_TILE);
+        if (inv_bytes) {
+            tc::bulk_load(Ahi, a.core_hi + cbase, inv_bytes, &bar_ld);
+            tc::bulk_load(Alo, a.core_lo + cbase, inv_bytes, &bar_ld);
+        }
+        if (q_bytes) {
+            const int64_t qoff = cbase + (int64_t)(ns8 + q0) * ns8;
+            tc::bulk_load(reinterpret_cast<unsigned char*>(Ahi) + qdst, a.core_hi + qoff, q_bytes, &bar_ld);
+            tc::bulk_load(reinterpret_cast<unsigned char*>(Alo) + qdst, a.core_lo + qoff, q_bytes, &bar_ld);
+        }
         tc::tma_load_2d(Tt, &rmap, k0, c0, &bar_ld);
         tc::tma_load_2d(Tt + 8192, &rmap, k0 + 32, c0, &bar_ld);
     }
     // the children's rows that land on this supernode's columns, while the TMA copies fly
     const GatherRange g1 = gather_open(a, fb, 0, ns, grs);
-    if (g1.E > 0) gather_issue<float, TCN, TCM>(a, g1, 0, k0, St, live);
+    if (g1.E > 0) gather_issue<float, TCN, TCF>(a, g1, 0, k0, St, live);
     copy_async_commit();
     bool ok = wait_all(&bar_ld, 0, &bail, a.err);
     if (ok) {
@@ -264,32 +284,37 @@ __global__ void __launch_bounds__(NT, 2) k_fwd_tc(SolveArgs<float> a, int32_t t0
         __syncthreads();
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_split_mma(tmem, Ahi, Alo, (uint32_t)(ns8 >> 2), false, Bhi, Blo, ns8 >> 3, false);
+            issue_split_mma<TCF>(tmem, Ahi, Alo, (uint32_t)(ns8 >> 2), false, Bhi, Blo, ns8 >> 3, false);
             tc::mma_commit(&bar_mma);
         }
-        // the children's rows of this chunk's update rows arrive while the product runs
+        // the children's rows of this task's update rows arrive while the product runs
         GatherRange g2{0, 0};
-        if (!xtask && nq > 0) {
+        if (nq > 0) {
             g2 = gather_open(a, fb, ns + q0, nq, grs);
-            if (g2.E > 0) gather_issue<float, TCN, TCM>(a, g2, 0, k0, St, live);
+            if (g2.E > 0) gather_issue<float, TCN, TCF>(a, g2, 0, k0, St, live);
             copy_async_commit();
         }
         ok = wait_all(&bar_mma, 0, &bail, a.err);
         if (ok) {
             tc::fence_after_sync();
+            // accumulator row r = TMEM lane r (M = 128): warp w reads lanes 32 (w % 4) .. + 31,
+            // columns 32 (w / 4) .. + 31
             float v[32];
-            acc_half(tmem, 0, v);
-            if (acc_lane()) {
-                float* o = Ot + acc_row() * TC_LS + acc_col();
+            const uint32_t base = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(32 * (warp >> 2));
+            tc::tmem_ld16(base, v);
+            tc::tmem_ld16(base + 16, v + 16);
+            {
+                float* o = Ot + (32 * (warp & 3) + lane) * TC_LS + 32 * (warp >> 2);
 #pragma unroll
                 for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
             }
             __syncthreads();
-            if (xtask) {
-                tile_rows_to_global<float, TCN>(a.B + (int64_t)c0 * K + k0, K, Ot, TC_LS, ns);
-            } else if (nq > 0) {
-                gather_finish<float, TCN, TCM, false>(a, g2, k0, Ot, TC_LS, nq, St, live, grs);
-                tile_rows_to_global<float, TCN>(a.U + (a.uoff[s] + q0) * (int64_t)K + k0, K, Ot, TC_LS, nq);
+            const int u0 = xtask ? 64 : 0;  // output-tile row of the first update row
+            if (xtask) tile_rows_to_global<float, TCN>(a.B + (int64_t)c0 * K + k0, K, Ot, TC_LS, ns);
+            if (nq > 0) {
+                gather_finish<float, TCN, TCF, false>(a, g2, k0, Ot + u0 * TC_LS, TC_LS, nq, St, live, grs);
+                tile_rows_to_global<float, TCN>(a.U + (a.uoff[s] + q0) * (int64_t)K + k0, K, Ot + u0 * TC_LS,
+                                                TC_LS, nq);
             }
         }
     }
@@ -401,7 +426,7 @@ __global__ void __launch_bounds__(NT, 2) k_bwd_tc(SolveArgs<float> a, int32_t t0
         __syncthreads();
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_split_mma(tmem, sAhi(b), sAlo(b), acores, true, sBhi(b), sBlo(b), (nc + 7) >> 3, j > 0);
+            issue_split_mma<TCM>(tmem, sAhi(b), sAlo(b), acores, true, sBhi(b), sBlo(b), (nc + 7) >> 3, j > 0);
             tc::mma_commit(&bar_mma[b]);
         }
     }
@@ -454,7 +479,7 @@ __global__ void __launch_bounds__(NT, 2) k_bwd_tc(SolveArgs<float> a, int32_t t0
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after_sync();
-                issue_split_mma(tmem + TCN, Fhi, Flo, acores, true, Bhi, Blo, ns8 >> 3, false);
+                issue_split_mma<TCM>(tmem + TCN, Fhi, Flo, acores, true, Bhi, Blo, ns8 >> 3, false);
                 tc::mma_commit(&bar_fin);
             }
             if ((ok = wait_all(&bar_fin, 1, &bail, a.err))) {
