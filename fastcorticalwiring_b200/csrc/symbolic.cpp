@@ -1,9 +1,10 @@
 // Symbolic sparse Cholesky analysis on the host.
 //
 // Ordering: geometric nested dissection. Each set of vertices is split at the
-// median of its projection on the principal axis of its coordinates; the
-// smaller one-sided boundary between the halves becomes the vertex separator,
-// numbered after both halves. Sets of at most `leaf_size` vertices are leaves.
+// median of its projection on one of eight directions (its coordinates'
+// principal axis, two directions orthogonal to it and their mixes), the one
+// whose smaller one-sided boundary between the halves is smallest; that boundary
+// becomes the vertex separator, numbered after both halves. Sets of at most `leaf_size` vertices are leaves.
 // The elimination tree is then postordered (same fill, contiguous subtrees),
 // and columns are grouped into supernodes:
 //   * relaxed supernodes: every maximal subtree of at most `relax` columns
@@ -82,6 +83,32 @@ void principal_axis(const double* X, const int32_t* v, int64_t n, double c[3], d
     for (int r = 0; r < 3; ++r) axis[r] = a[r] / na;
 }
 
+constexpr int kCandidates = 8;
+
+// The principal axis a, two unit directions orthogonal to it (p, q), and the mixes
+// (a +- p)/sqrt2, (a +- q)/sqrt2, (p +- q)/sqrt2 (the last pair only if room): 8 directions.
+void candidate_axes(const double a[3], double dirs[kCandidates][3]) {
+    double p[3];
+    // a vector not parallel to a, made orthogonal to it
+    const double e[3] = {std::fabs(a[0]) < 0.9 ? 1.0 : 0.0, std::fabs(a[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+    const double d = e[0] * a[0] + e[1] * a[1] + e[2] * a[2];
+    for (int k = 0; k < 3; ++k) p[k] = e[k] - d * a[k];
+    double np_ = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    for (int k = 0; k < 3; ++k) p[k] /= np_;
+    const double q[3] = {a[1] * p[2] - a[2] * p[1], a[2] * p[0] - a[0] * p[2], a[0] * p[1] - a[1] * p[0]};
+    const double r = 1.0 / std::sqrt(2.0);
+    for (int k = 0; k < 3; ++k) {
+        dirs[0][k] = a[k];
+        dirs[1][k] = p[k];
+        dirs[2][k] = q[k];
+        dirs[3][k] = (a[k] + p[k]) * r;
+        dirs[4][k] = (a[k] - p[k]) * r;
+        dirs[5][k] = (a[k] + q[k]) * r;
+        dirs[6][k] = (a[k] - q[k]) * r;
+        dirs[7][k] = (p[k] + q[k]) * r;
+    }
+}
+
 struct Dissector {
     const Graph& g;
     const double* X;
@@ -93,6 +120,28 @@ struct Dissector {
     Dissector(const Graph& g_, const double* X_, int leaf_)
         : g(g_), X(X_), leaf(leaf_), stamp(g_.n, 0), side(g_.n, 0) {}
 
+    // Size of the smaller one-sided boundary of the median split of proj (-1 if one side is empty).
+    int64_t separator_size(const int32_t* v, int64_t n, const std::vector<double>& proj, double med, int32_t id) {
+        int64_t n0 = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            side[v[i]] = proj[i] < med ? 0 : 1;
+            n0 += side[v[i]] == 0;
+        }
+        if (n0 == 0 || n0 == n) return -1;
+        int64_t s0 = 0, s1 = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const int32_t x = v[i];
+            for (int64_t k = g.xadj[x]; k < g.xadj[x + 1]; ++k) {
+                const int32_t y = g.adj[k];
+                if (stamp[y] == id && side[y] != side[x]) {
+                    (side[x] == 0 ? s0 : s1)++;
+                    break;
+                }
+            }
+        }
+        return std::min(s0, s1);
+    }
+
     // Writes an elimination order of v[0..n) into out[0..n).
     void dissect(const int32_t* v, int64_t n, int32_t* out) {
         if (n <= leaf) {
@@ -103,22 +152,44 @@ struct Dissector {
         for (int64_t i = 0; i < n; ++i) stamp[v[i]] = id;
         double c[3], ax[3];
         principal_axis(X, v, n, c, ax);
-        std::vector<double> proj(n);
+        // candidate cut directions: the principal axis, two directions orthogonal to it, and
+        // their half-way mixes; each is split at its median and the smallest separator wins
+        double dirs[kCandidates][3];
+        candidate_axes(ax, dirs);
+        std::vector<double> proj(n), tmp(n);
+        int64_t best_size = -1;
+        int best_dir = 0;
+        double best_med = 0.0;
+        for (int d = 0; d < kCandidates; ++d) {
+            const double* a = dirs[d];
+            for (int64_t i = 0; i < n; ++i) {
+                const double* x = X + 3 * (int64_t)v[i];
+                proj[i] = (x[0] - c[0]) * a[0] + (x[1] - c[1]) * a[1] + (x[2] - c[2]) * a[2];
+            }
+            tmp = proj;
+            std::nth_element(tmp.begin(), tmp.begin() + n / 2, tmp.end());
+            const double med = tmp[n / 2];
+            const int64_t sz = separator_size(v, n, proj, med, id);
+            if (sz >= 0 && (best_size < 0 || sz < best_size)) {
+                best_size = sz;
+                best_dir = d;
+                best_med = med;
+            }
+        }
+        if (best_size < 0) {
+            std::copy(v, v + n, out);
+            return;
+        }
         for (int64_t i = 0; i < n; ++i) {
             const double* x = X + 3 * (int64_t)v[i];
-            proj[i] = (x[0] - c[0]) * ax[0] + (x[1] - c[1]) * ax[1] + (x[2] - c[2]) * ax[2];
+            const double* a = dirs[best_dir];
+            proj[i] = (x[0] - c[0]) * a[0] + (x[1] - c[1]) * a[1] + (x[2] - c[2]) * a[2];
         }
-        std::vector<double> tmp(proj);
-        std::nth_element(tmp.begin(), tmp.begin() + n / 2, tmp.end());
-        double med = tmp[n / 2];
+        const double med = best_med;
         int64_t n0 = 0;
         for (int64_t i = 0; i < n; ++i) {
             side[v[i]] = proj[i] < med ? 0 : 1;
             n0 += side[v[i]] == 0;
-        }
-        if (n0 == 0 || n0 == n) {
-            std::copy(v, v + n, out);
-            return;
         }
         std::vector<int32_t> b0, b1;
         for (int64_t i = 0; i < n; ++i) {
