@@ -3,7 +3,8 @@
 Jobs (a cortical mesh, its scales, the sources to run) arrive at any time. Builder
 threads admit them when their device memory fits the budget (in arrival order,
 except that a job that fits may pass a head job waiting for memory a bounded
-number of times), prepare the mesh and factor it; the factors and the job's
+number of times; a job whose estimate exceeds the whole budget is refused with a
+result that carries the reason), prepare the mesh and factor it; the factors and the job's
 right-hand-side blocks stay resident until the job is done. The dispatch loop
 keeps the next chunk of source blocks of the few admitted jobs with the least
 work left enqueued on each job's own stream, so their blocks overlap on the
@@ -55,6 +56,7 @@ class JobResult:
     n_vertices: int
     estimate_bytes: int = 0
     engine_info: dict | None = None
+    error: str | None = None  # set when the job was refused (no records)
 
     @property
     def latency_s(self) -> float:
@@ -262,6 +264,9 @@ class Server:
         """The next job to admit (caller holds the lock): the head of the queue if it fits
         the budget (or nothing is resident); else the first later job that fits, while the
         head has been passed fewer than max_bypass times."""
+        # a job whose estimate exceeds the whole budget can never be admitted: refuse it
+        while self._pending and self._estimate(self._pending[0]) > self.budget:
+            self._refuse(self._pending.popleft())
         if not self._pending:
             return None
         head = self._pending[0]
@@ -277,6 +282,16 @@ class Server:
                 self._bypassed += 1
                 return q
         return None
+
+    def _refuse(self, p: _Pending) -> None:
+        """Record a job that cannot fit the HBM budget (caller holds the lock)."""
+        now = time.perf_counter()
+        msg = (f"job {p.job.job_id!r} needs an estimated {p.estimate / 1e9:.2f} GB of device memory, more than "
+               f"the {self.budget / 1e9:.2f} GB budget")
+        self.results[p.job.job_id] = JobResult(p.job.job_id, np.zeros(0, np.int32), np.zeros((0, 0)), p.t_arrive,
+                                               now, now, 0, 0, p.estimate, None, error=msg)
+        self._n_open -= 1
+        self._cv.notify_all()
 
     def _admit(self, p: _Pending) -> _Active:
         torch = self.torch

@@ -18,6 +18,8 @@ def _server(budget, max_bypass=2):
     srv._pending = deque()
     srv._reserved = 0
     srv._bypassed = 0
+    srv.results = {}
+    srv._n_open = 0
     return srv
 
 
@@ -51,3 +53,16 @@ def test_memory_estimate_grows_with_the_job():
     assert e(160_000, 320_000, 1024, 2, 160_000, S._stride(12, 3)) > 3 * base
     assert e(40_000, 80_000, 1024, 4, 40_000, S._stride(12, 3)) > base
     assert e(40_000, 80_000, 512, 2, 40_000, S._stride(12, 3)) < base
+
+
+def test_job_larger_than_the_budget_is_refused_not_run():
+    """A job that can never fit the HBM budget gets a result with the reason (no records), and the
+    jobs behind it are admitted as usual."""
+    srv = _server(budget=100)
+    srv._pending.extend([_pending("huge", 150), _pending("a", 20)])
+    srv._n_open = 2
+    with srv._cv:  # the builders call _pick holding the lock
+        assert srv._pick().job.job_id == "a"
+    r = srv.results["huge"]
+    assert r.error is not None and "budget" in r.error and r.records.size == 0
+    assert srv._n_open == 1
