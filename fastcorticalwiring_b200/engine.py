@@ -304,6 +304,17 @@ def create_distance_engine(engine_type, vertices, faces, engine_kwargs=None):
     return ENGINE_REGISTRY[key](vertices, faces, **dict(engine_kwargs or {}))
 
 
-def register(registry: dict) -> None:
-    """Add the b200 engine to another registry (e.g. distance_engines.ENGINE_REGISTRY)."""
-    registry["b200"] = B200DistanceEngine
+def engine_class(base=None):
+    """B200DistanceEngine, or a subclass of it that is also a subclass of `base` (the host
+    application's own engine ABC, e.g. distance_engines.BaseDistanceEngine), so isinstance
+    checks against the host's contract hold."""
+    if base is None or issubclass(B200DistanceEngine, base):
+        return B200DistanceEngine
+    return type("B200DistanceEngine", (B200DistanceEngine, base),
+                {"__module__": __name__, "__doc__": B200DistanceEngine.__doc__})
+
+
+def register(registry: dict, base=None) -> None:
+    """Add the b200 engine to another registry (e.g. distance_engines.ENGINE_REGISTRY), as a
+    subclass of `base` when given (e.g. distance_engines.BaseDistanceEngine)."""
+    registry["b200"] = engine_class(base)

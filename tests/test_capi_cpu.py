@@ -129,3 +129,31 @@ def test_record_layout_matches_the_header():
         if ne:
             assert r["extra_a"][0, -1] == stride - 1
     assert _lib.samples_capacity(32, 8) == 32 + 31 * 8
+
+
+def test_registered_engine_subclasses_the_host_contract():
+    """register(registry, base) installs a class that is also a subclass of the host's own engine ABC
+    (distance_engines.BaseDistanceEngine in the reference), so isinstance checks there hold."""
+    from abc import ABC, abstractmethod
+
+    class HostBase(ABC):  # the shape of distance_engines.py:54-69
+        def __init__(self, vertices, faces, **engine_kwargs):
+            self.engine_kwargs = dict(engine_kwargs)
+
+        @property
+        @abstractmethod
+        def name(self):
+            raise NotImplementedError
+
+        @abstractmethod
+        def compute_distance(self, source_idx):
+            raise NotImplementedError
+
+    reg = {}
+    engine.register(reg, base=HostBase)
+    cls = reg["b200"]
+    assert issubclass(cls, HostBase) and issubclass(cls, engine.B200DistanceEngine)
+    assert engine.engine_class() is engine.B200DistanceEngine
+    z, pm = _l4()
+    with pytest.raises(_lib.FCWError):  # no device here: construction reaches the engine and fails loudly
+        cls(pm.V, pm.F)
