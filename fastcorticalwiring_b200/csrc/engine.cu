@@ -169,7 +169,7 @@ struct fcw_engine {
     double *val_h = nullptr, *inv_h = nullptr, *val_p = nullptr, *inv_p = nullptr;
     float *val_g = nullptr, *inv_g = nullptr;
     // tensor-core FP32 sweeps: core arrays of the grounded factor and the forward task list
-    float *core_hi = nullptr, *core_lo = nullptr;
+    float *core_hi = nullptr, *core_lo = nullptr, *coreT_hi = nullptr, *coreT_lo = nullptr;
     int64_t* core_ptr_d = nullptr;
     int2* tc_fwd_tasks = nullptr;
     std::vector<int32_t> tc_fwd_ptr;
@@ -663,7 +663,10 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
             FCW_TRY(e->upload(&e->core_ptr_d, cptr));
             FCW_TRY(e->dalloc(&e->core_hi, (size_t)cptr[S.nsuper]));
             FCW_TRY(e->dalloc(&e->core_lo, (size_t)cptr[S.nsuper]));
-            fcw::launch_build_cores(e->plan, val_tmp, inv_tmp, e->core_ptr_d, e->core_hi, e->core_lo, e->stream);
+            FCW_TRY(e->dalloc(&e->coreT_hi, (size_t)cptr[S.nsuper]));
+            FCW_TRY(e->dalloc(&e->coreT_lo, (size_t)cptr[S.nsuper]));
+            fcw::launch_build_cores(e->plan, val_tmp, inv_tmp, e->core_ptr_d, e->core_hi, e->core_lo, e->coreT_hi,
+                                    e->coreT_lo, e->stream);
             FCW_CUDA(cudaGetLastError());
         }
         FCW_CUDA(cudaStreamSynchronize(e->stream));
@@ -765,6 +768,8 @@ fcw::SolveArgs<T> solve_args(fcw_engine* e, const T* val, const T* inv, T* B, in
     a.ktiles = e->cw().K / fcw::kRhsTile;
     a.core_hi = e->core_hi;
     a.core_lo = e->core_lo;
+    a.coreT_hi = e->coreT_hi;
+    a.coreT_lo = e->coreT_lo;
     a.core_ptr = e->core_ptr_d;
     a.err = e->err_d;
     return a;

@@ -88,6 +88,8 @@ struct SolveArgs {
     // round_up(nr, 32) rows (padding zero)
     const float* core_hi = nullptr;
     const float* core_lo = nullptr;
+    const float* coreT_hi = nullptr;     // the transposes (backward products), 32-row chunks
+    const float* coreT_lo = nullptr;
     const int64_t* core_ptr = nullptr;   // per supernode: offset (floats) of its core array
     int* err = nullptr;                  // error bits (bounded waits that expired)
 };
@@ -119,7 +121,7 @@ cudaError_t configure_tc_kernels();
 int make_rows_map(CUtensorMap* map, const float* base, int64_t n, int32_t K);
 // The core arrays of the tensor-core sweeps from the FP64 panels and inverse blocks.
 void launch_build_cores(const DevPlan& p, const double* val, const double* inv, const int64_t* core_ptr,
-                        float* hi, float* lo, cudaStream_t st);
+                        float* hi, float* lo, float* hiT, float* loT, cudaStream_t st);
 
 // ---- fused gradient -> normalise -> divergence (face.cu) ----
 struct FaceData {

@@ -7,18 +7,22 @@
 //   * Each FP32 operand is split into two TF32 terms (hi = rna(x), lo =
 //     rna(x - hi)) and hi*hi + hi*lo + lo*hi accumulate, which keeps the product
 //     at FP32 accuracy (the dropped lo*lo term is below 2^-22 |a||b|).
+//   * Every operand is K-major (the product's depth contiguous in 16-byte
+//     chunks of core matrices; tc.cuh): a transposed, MN-major operand read as
+//     kind::tf32 with no swizzle comes back as zeros on this hardware, so the
+//     transposes are made when the operands are written instead.
 //   * The panel operands are prepared once per factorisation: the stacked
-//     [inv(L_ss); Q_s] of each supernode, split into hi and lo arrays in the
-//     tensor core's core-matrix order (tc.cuh). A task's 64-row slice is one
-//     contiguous range, fetched by the TMA engine as two bulk copies. The same
-//     array read with its strides swapped is the transposed operand of the
-//     backward sweep (Q_s^T, inv(L_ss)^T).
+//     [inv(L_ss); Q_s] of each supernode, split into hi and lo arrays in
+//     core-matrix order, once as stored (rows x columns, the forward's A) and
+//     once transposed in 32-row chunks (the backward's A = Q_s^T, inv(L_ss)^T).
+//     A task's slice is one contiguous range, fetched by the TMA engine as two
+//     bulk copies.
 //   * A supernode's own right-hand-side rows (forward: R, backward: y_s) are a
 //     64-row x 64-column box of the n x K array, fetched by a tiled TMA load with
 //     128-byte swizzle; children's update rows and ancestors' solution rows are
 //     gathered by index with 16-byte cp.async copies, as in solve.cu.
-//   * Threads split the right-hand-side tile into TF32 terms in the core-matrix
-//     layout, one thread issues the MMAs, a tcgen05.commit arrives on an
+//   * Threads split the right-hand-side tile into TF32 terms, transposed into the
+//     K-major core-matrix layout, one thread issues the MMAs, a tcgen05.commit arrives on an
 //     mbarrier, and the accumulator comes back through tcgen05.ld to a shared
 //     tile that is written out with 16-byte row-segment stores.
 //
@@ -40,7 +44,9 @@ constexpr int TCF = 128;                // rows of a forward task's product (M =
 constexpr int TC_RC = 32;               // structure rows per backward chunk
 constexpr int TC_PT = kMaxWidth;        // rows of a backward partial-sum slot
 constexpr uint32_t TC_TILE = 64u * TCN * 4u;   // a 64 x 64 FP32 tile (16 KB)
-constexpr uint32_t TC_SLACK = 2048;     // an MN-major A of M = 64 reads up to 2 KB past its last row group
+// A backward A of M = 64 (8 groups of 8 columns) holds only ns8 / 8 groups: the product reads up to
+// 7 groups of 8 k-chunks (7 KB) past a chunk tile, 4 KB past the inverse block's tile
+constexpr uint32_t TC_SLACK = 7168;
 
 // Byte offset of element (r, c) of the own-row tile: two TMA boxes of 64 rows x 32
 // columns (128-byte rows), 128-byte swizzle (16-byte chunk index XOR row % 8).
@@ -90,28 +96,35 @@ __device__ __forceinline__ void gather_finish_swz(const SolveArgs<float>& a, con
     } while (e0 < g.E);
 }
 
-// Rows [0, nk) of the swizzled own-row tile as the MN-major B operand (K = round_up(nk, 8)
-// rows, rows >= nk zero), split into TF32 hi and lo. B hi overlays the tile, so every
-// thread reads its values before any thread writes. Item i: (k-group, 4-column chunk,
-// row in core) with the row fastest, so 8 lanes fill one 128-byte core and read 8
-// distinct swizzled chunks.
+// Rows [0, nk) of the swizzled own-row tile (k x 64 columns) as the K-major B operand:
+// element (n, k) at core (n / 8, k / 4) of round_up(nk, 8) / 4 k-chunks per 8-column group,
+// split into TF32 hi and lo; rows k >= nk are zero. B hi overlays the tile, so every thread
+// reads its values before any thread writes. Item i = (k-chunk, column group, column in
+// group) with the column fastest: a warp reads 32 consecutive columns of a row (conflict
+// free under the swizzle) and 8 lanes fill one 128-byte core.
 __device__ __forceinline__ void split_own_rows(const unsigned char* Tt, int nk, float* Bhi, float* Blo) {
     constexpr int PER = (64 * TCN / 4) / NT;
-    const int nk8 = (nk + 7) & ~7;
+    const int nk8 = (nk + 7) & ~7, kcores = nk8 >> 2;
     float4 w[PER];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const int i = threadIdx.x + j * NT;
-        const int kk = i & 7, c = (i >> 3) & 15, k = ((i >> 7) << 3) + kk;
-        w[j] = k < nk ? *reinterpret_cast<const float4*>(Tt + swz(k, 4 * c)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int n = i & 63, kc = i >> 6;
+        float x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = 4 * kc + q;
+            x[q] = k < nk ? *reinterpret_cast<const float*>(Tt + swz(k, n)) : 0.0f;
+        }
+        w[j] = make_float4(x[0], x[1], x[2], x[3]);
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const int i = threadIdx.x + j * NT;
-        const int kk = i & 7, c = (i >> 3) & 15, kg = i >> 7;
-        if (kg * 8 >= nk8) continue;
-        const uint32_t off = ((uint32_t)(kg * 16 + c) << 5) + (uint32_t)(kk << 2);  // floats
+        const int n = i & 63, kc = i >> 6;
+        if (kc >= kcores) continue;
+        const uint32_t off = ((uint32_t)((n >> 3) * kcores + kc) << 5) + (uint32_t)((n & 7) << 2);  // floats
         float4 h, l;
         tc::split_tf32(w[j].x, h.x, l.x);
         tc::split_tf32(w[j].y, h.y, l.y);
@@ -122,45 +135,48 @@ __device__ __forceinline__ void split_own_rows(const unsigned char* Tt, int nk, 
     }
 }
 
-// Rows [0, nk) of a gathered-row tile (row stride TC_LS) as the MN-major B operand of
-// TC_RC rows (rows >= nk zero), split into TF32 hi and lo (separate buffers).
+// Rows [0, nk) of a gathered-row tile (TC_RC rows x 64 columns, row stride TC_LS) as the
+// K-major B operand of TC_RC rows (8 k-chunks per 8-column group; rows >= nk zero), split
+// into TF32 hi and lo (separate buffers).
 __device__ __forceinline__ void split_gathered(const float* Xg, int nk, float* Bhi, float* Blo) {
-    constexpr int PER = (TC_RC * TCN / 4) / NT;
+    constexpr int PER = (TC_RC * TCN / 4) / NT, KC = TC_RC / 4;
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const int i = threadIdx.x + j * NT;
-        const int kk = i & 7, c = (i >> 3) & 15, kg = i >> 7, k = kg * 8 + kk;
-        const float4 w = k < nk ? *reinterpret_cast<const float4*>(Xg + k * TC_LS + 4 * c)
-                                : make_float4(0.f, 0.f, 0.f, 0.f);
-        const uint32_t off = ((uint32_t)(kg * 16 + c) << 5) + (uint32_t)(kk << 2);
+        const int n = i & 63, kc = i >> 6;
+        float x[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = 4 * kc + q;
+            x[q] = k < nk ? Xg[k * TC_LS + n] : 0.0f;
+        }
+        const uint32_t off = ((uint32_t)((n >> 3) * KC + kc) << 5) + (uint32_t)((n & 7) << 2);
         float4 h, l;
-        tc::split_tf32(w.x, h.x, l.x);
-        tc::split_tf32(w.y, h.y, l.y);
-        tc::split_tf32(w.z, h.z, l.z);
-        tc::split_tf32(w.w, h.w, l.w);
+        tc::split_tf32(x[0], h.x, l.x);
+        tc::split_tf32(x[1], h.y, l.y);
+        tc::split_tf32(x[2], h.z, l.z);
+        tc::split_tf32(x[3], h.w, l.w);
         *reinterpret_cast<float4*>(Bhi + off) = h;
         *reinterpret_cast<float4*>(Blo + off) = l;
     }
 }
 
-// D (+)= A B (M rows) over ksteps steps of K = 8 with two TF32 terms per operand. A is K-major
-// (a_mn = false: 8-row groups a_sbo apart, k-chunks 128 bytes apart, 256 bytes per step)
-// or MN-major (a_mn = true: the transposed read of a core array, 4-column chunks 128 bytes
-// apart, k-groups a_lbo apart, one group per step). B is MN-major with 16 n-chunks.
+// D (+)= A B (M rows, N = 64) over ksteps steps of K = 8 with two TF32 terms per operand.
+// Both operands K-major: A in groups of 8 rows with a_kcores 16-byte k-chunks each, B in
+// groups of 8 columns with b_kcores k-chunks each; a step advances both by two chunks.
 template <int M>
-__device__ __forceinline__ void issue_split_mma(uint32_t d, const float* Ahi, const float* Alo, uint32_t a_cores,
-                                                bool a_mn, const float* Bhi, const float* Blo, int ksteps,
+__device__ __forceinline__ void issue_split_mma(uint32_t d, const float* Ahi, const float* Alo, uint32_t a_kcores,
+                                                const float* Bhi, const float* Blo, uint32_t b_kcores, int ksteps,
                                                 bool accumulate) {
-    const uint32_t idesc = tc::idesc_tf32(M, TCN, a_mn, true, false);
+    const uint32_t idesc = tc::idesc_tf32(M, TCN, false, false, false);
     const uint32_t ah = tc::smem_u32(Ahi), al = tc::smem_u32(Alo), bh = tc::smem_u32(Bhi), bl = tc::smem_u32(Blo);
-    const uint32_t a_lbo = a_mn ? a_cores * 128u : 128u, a_sbo = a_mn ? 128u : a_cores * 128u;
-    const uint32_t a_step = a_mn ? a_cores * 128u : 256u;
-    constexpr uint32_t b_lbo = (TCN / 4) * 128u, b_sbo = 128u;
+    const uint32_t a_sbo = a_kcores * 128u, b_sbo = b_kcores * 128u;
     for (int ks = 0; ks < ksteps; ++ks) {
-        const uint64_t dah = tc::sdesc(ah + ks * a_step, a_lbo, a_sbo);
-        const uint64_t dal = tc::sdesc(al + ks * a_step, a_lbo, a_sbo);
-        const uint64_t dbh = tc::sdesc(bh + ks * b_lbo, b_lbo, b_sbo);
-        const uint64_t dbl = tc::sdesc(bl + ks * b_lbo, b_lbo, b_sbo);
+        const uint32_t step = (uint32_t)ks * 256u;
+        const uint64_t dah = tc::sdesc(ah + step, 128u, a_sbo);
+        const uint64_t dal = tc::sdesc(al + step, 128u, a_sbo);
+        const uint64_t dbh = tc::sdesc(bh + step, 128u, b_sbo);
+        const uint64_t dbl = tc::sdesc(bl + step, 128u, b_sbo);
         tc::mma_tf32(d, dah, dbh, idesc, (accumulate || ks > 0) ? 1u : 0u);
         tc::mma_tf32(d, dah, dbl, idesc, 1u);
         tc::mma_tf32(d, dal, dbh, idesc, 1u);
@@ -284,7 +300,8 @@ __global__ void __launch_bounds__(NT, 2) k_fwd_tc(SolveArgs<float> a, int32_t t0
         __syncthreads();
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_split_mma<TCF>(tmem, Ahi, Alo, (uint32_t)(ns8 >> 2), false, Bhi, Blo, ns8 >> 3, false);
+            issue_split_mma<TCF>(tmem, Ahi, Alo, (uint32_t)(ns8 >> 2), Bhi, Blo, (uint32_t)(ns8 >> 2), ns8 >> 3,
+                                 false);
             tc::mma_commit(&bar_mma);
         }
         // the children's rows of this task's update rows arrive while the product runs
@@ -394,9 +411,9 @@ __global__ void __launch_bounds__(NT, 2) k_bwd_tc(SolveArgs<float> a, int32_t t0
         const int b = j & 1, qq = q0 + j * TC_RC, nc = min(TC_RC, q1 - qq);
         if (tid == 0) {
             tc::mbar_arrive_expect_tx(&bar_ld[b], 2 * cbytes);
-            const int64_t off = cbase + (int64_t)(ns8 + qq) * ns8;
-            tc::bulk_load(sAhi(b), a.core_hi + off, cbytes, &bar_ld[b]);
-            tc::bulk_load(sAlo(b), a.core_lo + off, cbytes, &bar_ld[b]);
+            const int64_t off = cbase + (int64_t)(ns8 + qq) * ns8;  // chunk qq / 32 of the transposed array
+            tc::bulk_load(sAhi(b), a.coreT_hi + off, cbytes, &bar_ld[b]);
+            tc::bulk_load(sAlo(b), a.coreT_lo + off, cbytes, &bar_ld[b]);
         }
         float* Xg = sXg(b);
         for (int i = tid; i < nc * (TCN / 4); i += NT) {
@@ -426,7 +443,8 @@ __global__ void __launch_bounds__(NT, 2) k_bwd_tc(SolveArgs<float> a, int32_t t0
         __syncthreads();
         if (tid == 0) {
             tc::fence_after_sync();
-            issue_split_mma<TCM>(tmem, sAhi(b), sAlo(b), acores, true, sBhi(b), sBlo(b), (nc + 7) >> 3, j > 0);
+            issue_split_mma<TCM>(tmem, sAhi(b), sAlo(b), TC_RC / 4, sBhi(b), sBlo(b), TC_RC / 4, (nc + 7) >> 3,
+                                 j > 0);
             tc::mma_commit(&bar_mma[b]);
         }
     }
@@ -467,8 +485,8 @@ __global__ void __launch_bounds__(NT, 2) k_bwd_tc(SolveArgs<float> a, int32_t t0
         if (tid == 0) {
             const uint32_t ibytes = (uint32_t)ns8 * (uint32_t)ns8 * 4u;
             tc::mbar_arrive_expect_tx(&bar_fin, 2 * ibytes + TC_TILE);
-            tc::bulk_load(Fhi, a.core_hi + cbase, ibytes, &bar_fin);
-            tc::bulk_load(Flo, a.core_lo + cbase, ibytes, &bar_fin);
+            tc::bulk_load(Fhi, a.coreT_hi + cbase, ibytes, &bar_fin);
+            tc::bulk_load(Flo, a.coreT_lo + cbase, ibytes, &bar_fin);
             tc::tma_load_2d(Tt, &bmap, k0, c0, &bar_fin);
             tc::tma_load_2d(Tt + 8192, &bmap, k0 + 32, c0, &bar_fin);
         }
@@ -479,7 +497,7 @@ __global__ void __launch_bounds__(NT, 2) k_bwd_tc(SolveArgs<float> a, int32_t t0
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after_sync();
-                issue_split_mma<TCM>(tmem + TCN, Fhi, Flo, acores, true, Bhi, Blo, ns8 >> 3, false);
+                issue_split_mma<TCM>(tmem + TCN, Fhi, Flo, acores, Bhi, Blo, acores, ns8 >> 3, false);
                 tc::mma_commit(&bar_fin);
             }
             if ((ok = wait_all(&bar_fin, 1, &bail, a.err))) {
@@ -530,18 +548,23 @@ __global__ void __launch_bounds__(NT, 2) k_bwd_tc(SolveArgs<float> a, int32_t t0
     if (warp == 0) tc::tmem_dealloc(tmem, 2 * TCN);
 }
 
-// Core arrays of the stacked [inv(L_ss); Q_s], one CTA per supernode: element (row, col)
-// at core_offset(row, col, ns8 / 4); rows >= ns of the inverse part, rows >= nr of the Q
-// part and columns >= ns are zero. hi = rna_tf32(x), lo = rna_tf32(x - hi) from the FP64 value.
+// Core arrays of the stacked [inv(L_ss); Q_s], one CTA per supernode (rows >= ns of the
+// inverse part, rows >= nr of the Q part and columns >= ns are zero; hi = rna_tf32(x),
+// lo = rna_tf32(x - hi) from the FP64 value):
+//  * forward (hi, lo): element (row r, column i) at core_offset(r, i, ns8 / 4), the K-major
+//    A of the forward products (rows x columns);
+//  * backward (hiT, loT): the transposes, K-major over the rows: the inverse part
+//    (rows j < ns8) at core_offset(i, j, ns8 / 4), then each 32-row chunk of Q_s (local row
+//    q) at ns8 * ns8 + chunk * 32 * ns8 floats + core_offset(i, q, 8).
 __global__ void k_build_cores(DevPlan p, const double* __restrict__ val, const double* __restrict__ inv,
-                              const int64_t* __restrict__ core_ptr, float* __restrict__ hi, float* __restrict__ lo) {
+                              const int64_t* __restrict__ core_ptr, float* __restrict__ hi, float* __restrict__ lo,
+                              float* __restrict__ hiT, float* __restrict__ loT) {
     const int s = blockIdx.x;
     const int c0 = p.sn_c0[s], ns = p.sn_c0[s + 1] - c0, nr = p.sn_m[s] - ns;
     const int ns8 = (ns + 7) & ~7, nr32 = (nr + 31) & ~31, rows = ns8 + nr32;
     const double* P = val + p.sn_valptr[s];
     const double* I = inv + p.sn_invptr[s];
-    float* H = hi + core_ptr[s];
-    float* L = lo + core_ptr[s];
+    const int64_t base = core_ptr[s];
     const int icores = ns8 >> 2;
     for (int e = threadIdx.x; e < rows * ns8; e += blockDim.x) {
         const int r = e / ns8, c = e - r * ns8;
@@ -552,9 +575,18 @@ __global__ void k_build_cores(DevPlan p, const double* __restrict__ val, const d
         }
         const float h = tc::to_tf32((float)x);
         const float l = tc::to_tf32((float)(x - (double)h));
-        const uint32_t off = tc::core_offset(r, c, icores) >> 2;
-        H[off] = h;
-        L[off] = l;
+        const int64_t off = base + (tc::core_offset(r, c, icores) >> 2);
+        hi[off] = h;
+        lo[off] = l;
+        int64_t offT;
+        if (r < ns8) {
+            offT = base + (tc::core_offset(c, r, icores) >> 2);
+        } else {
+            const int q = r - ns8;
+            offT = base + (int64_t)ns8 * ns8 + (int64_t)(q >> 5) * 32 * ns8 + (tc::core_offset(c, q & 31, 8) >> 2);
+        }
+        hiT[offT] = h;
+        loT[offT] = l;
     }
 }
 
@@ -583,9 +615,9 @@ void launch_bwd_level_tc(const SolveArgs<float>& a, int32_t t0, int32_t ntasks, 
 }
 
 void launch_build_cores(const DevPlan& p, const double* val, const double* inv, const int64_t* core_ptr, float* hi,
-                        float* lo, cudaStream_t st) {
+                        float* lo, float* hiT, float* loT, cudaStream_t st) {
     if (p.nsuper <= 0) return;
-    k_build_cores<<<p.nsuper, 256, 0, st>>>(p, val, inv, core_ptr, hi, lo);
+    k_build_cores<<<p.nsuper, 256, 0, st>>>(p, val, inv, core_ptr, hi, lo, hiT, loT);
 }
 
 int make_rows_map(CUtensorMap* map, const float* base, int64_t n, int32_t K) {

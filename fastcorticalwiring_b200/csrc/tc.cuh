@@ -2,18 +2,15 @@
 // products with TMEM accumulators, TMA bulk copies completing on mbarriers,
 // and the split of FP32 operands into two TF32 terms.
 //
-// Operand layouts are the "no swizzle" canonical layouts of the UMMA shared
-// memory descriptor. The unit is a core matrix of 128 contiguous bytes:
-// 8 rows of 16 bytes (4 FP32/TF32 values).
-//   * K-major (A = M x K, K contiguous): core (m/8, k/4) holds rows m%8, each
-//     with 4 consecutive k. LBO = byte stride between k-chunks of 4, SBO =
-//     byte stride between groups of 8 rows.
-//   * MN-major (B = K x N, N contiguous): core (k/8, n/4) holds 8 k-rows, each
-//     with 4 consecutive n. LBO = byte stride between groups of 8 k, SBO =
-//     byte stride between n-chunks of 4.
-// Both place element (outer8, inner4) of a core matrix at byte
-// (outer8 % 8) * 16 + (inner4 % 4) * 4, so one array of cores serves as a
-// K-major A and, read with LBO and SBO swapped, as the MN-major transpose.
+// Operands use the "no swizzle" K-major canonical layout of the UMMA shared
+// memory descriptor. The unit is a core matrix of 128 contiguous bytes: 8 rows
+// (of A) or 8 columns (of B) of 16 bytes, each holding 4 consecutive depth (k)
+// values. LBO = byte stride between the 16-byte k-chunks of a group (128 here:
+// a group's chunks are consecutive cores), SBO = byte stride between groups of 8
+// rows or columns. Element (outer, k) of an array of cores ordered group-major is
+// at core_offset(outer, k, k-chunks per group). (The transposed, MN-major
+// operand read of kind::tf32 without swizzle returned zeros on B200, so the
+// sweeps transpose an operand when they write it instead.)
 #pragma once
 
 #include <cuda.h>
@@ -38,7 +35,8 @@ __device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
 }
 
 // Byte offset of element (outer, inner) in a core-matrix array whose cores are
-// ordered outer-group major: core (outer/8, inner/4) at index (outer/8) * icores + inner/4.
+// ordered outer-group major: core (outer/8, inner/4) at index (outer/8) * icores + inner/4
+// (inner is the product's depth k).
 __host__ __device__ __forceinline__ uint32_t core_offset(int outer, int inner, int icores) {
     return (uint32_t)((((outer >> 3) * icores + (inner >> 2)) << 7) + ((outer & 7) << 4) + ((inner & 3) << 2));
 }
@@ -90,18 +88,33 @@ __device__ __forceinline__ void tmem_relinquish() {
 __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
-// 32 lanes x 16 consecutive columns: thread i of the warp gets lane (taddr.lane + i).
+// 32 lanes x 16 consecutive columns: thread i of the warp gets lane (taddr.lane + i). The
+// load and its wait are one asm statement, so the registers are complete when it returns.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     uint32_t r[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
+        "%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        : "r"(taddr)
+        : "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+// The same shape, registers -> tensor memory, completed before it returns.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float* v) {
+    uint32_t r[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r[i] = __float_as_uint(v[i]);
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};\n\t"
+        "tcgen05.wait::st.sync.aligned;" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
 }
 
 // ---- mbarriers ----

@@ -15,7 +15,8 @@ constexpr int kCheckThreads = 256;
 
 // One CTA. A: M x Kd row-major (trans = 0), or P: Kd x M row-major read as P^T
 // (trans = 1). B: Kd x N row-major. C: M x N row-major. terms: 1 (hi x hi) or
-// 3 (hi x hi + hi x lo + lo x hi). M <= 128, Kd <= 64, N in {64, 128}.
+// 3 (hi x hi + hi x lo + lo x hi); 0 and 2 are checks of the accumulator paths (see
+// below). M <= 128, Kd <= 64, N in {64, 128}.
 __global__ void __launch_bounds__(kCheckThreads) k_tc_product(const float* __restrict__ A,
                                                              const float* __restrict__ B, float* __restrict__ C,
                                                              int M, int Kd, int N, int terms, int trans,
@@ -26,25 +27,22 @@ __global__ void __launch_bounds__(kCheckThreads) k_tc_product(const float* __res
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int MM = M <= 64 ? 64 : 128;          // instruction M
     const int Kp = (Kd + 7) / 8 * 8;            // depth padded to the instruction's K = 8
-    // A tile: MM rows (trans: MM columns of P) x Kp, hi and lo; slack for the MN-major read
-    const int a_cores = trans ? (MM / 4) : (Kp / 4);  // inner cores per outer group of 8
-    const int a_outer = trans ? Kp : MM;
-    const uint32_t a_bytes = (uint32_t)(a_outer / 8) * a_cores * 128u;
+    const int kcores = Kp / 4;                  // 16-byte k-chunks per 8-row (8-column) group
+    // both operands K-major, as in the sweeps: A (MM rows; trans: the transpose of P, made
+    // when it is written) and B^T (N columns), split into TF32 hi and lo, zero outside
+    const uint32_t a_bytes = (uint32_t)MM * Kp * 4u;
+    const uint32_t b_bytes = (uint32_t)N * Kp * 4u;
     float* Ahi = reinterpret_cast<float*>(sm);
     float* Alo = reinterpret_cast<float*>(sm + a_bytes);
-    const int b_cores = N / 4;
-    const uint32_t b_bytes = (uint32_t)(Kp / 8) * b_cores * 128u;
     float* Bhi = reinterpret_cast<float*>(sm + 2 * a_bytes);
     float* Blo = reinterpret_cast<float*>(sm + 2 * a_bytes + b_bytes);
-    // operands split into TF32 terms, zero outside the matrices
-    for (int e = tid; e < a_outer * a_cores * 4; e += kCheckThreads) {
-        const int o = e / (a_cores * 4), i = e - o * (a_cores * 4);
+    for (int e = tid; e < MM * Kp; e += kCheckThreads) {
+        const int m = e / Kp, k = e - m * Kp;
         float x = 0.0f;
-        if (!trans && o < M && i < Kd) x = A[o * Kd + i];
-        if (trans && o < Kd && i < M) x = A[o * M + i];
+        if (m < M && k < Kd) x = trans ? A[k * M + m] : A[m * Kd + k];
         float hi, lo;
         tc::split_tf32(x, hi, lo);
-        const uint32_t off = tc::core_offset(o, i, a_cores) >> 2;
+        const uint32_t off = tc::core_offset(m, k, kcores) >> 2;
         Ahi[off] = hi;
         Alo[off] = lo;
     }
@@ -53,7 +51,7 @@ __global__ void __launch_bounds__(kCheckThreads) k_tc_product(const float* __res
         const float x = k < Kd ? B[k * N + n] : 0.0f;
         float hi, lo;
         tc::split_tf32(x, hi, lo);
-        const uint32_t off = tc::core_offset(k, n, b_cores) >> 2;
+        const uint32_t off = tc::core_offset(n, k, kcores) >> 2;
         Bhi[off] = hi;
         Blo[off] = lo;
     }
@@ -67,22 +65,31 @@ __global__ void __launch_bounds__(kCheckThreads) k_tc_product(const float* __res
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = tbase;
-    if (tid == 0) {
-        const uint32_t idesc = tc::idesc_tf32(MM, N, trans != 0, true, false);
-        // K-major A: SBO = stride of 8-row groups, LBO = stride of 4-wide k chunks.
-        // MN-major A (P^T): SBO = stride of 4-wide m chunks, LBO = stride of 8-row k groups.
-        const uint32_t a_lbo = trans ? (uint32_t)a_cores * 128u : 128u;
-        const uint32_t a_sbo = trans ? 128u : (uint32_t)a_cores * 128u;
-        const uint32_t a_step = trans ? (uint32_t)a_cores * 128u : 256u;  // bytes per k-step of 8
-        const uint32_t b_lbo = (uint32_t)b_cores * 128u, b_sbo = 128u, b_step = b_lbo;
+    // terms 0 / 2: lane l, column c of the accumulator first set to l * 1024 + c by tcgen05.st
+    // (0: nothing else, a check of the accumulator's store and load paths; 2: the one-term
+    // product is then added to it)
+    if ((terms == 0 || terms == 2) && warp < 4) {
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            float v[16];
+            for (int j = 0; j < 16; ++j) v[j] = (float)((32 * warp + lane) * 1024 + c0 + j);
+            tc::tmem_st16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (tid == 0 && terms != 0) {
+        const uint32_t idesc = tc::idesc_tf32(MM, N, false, false, false);
+        const uint32_t sbo = (uint32_t)kcores * 128u;  // 8-row groups; k-chunks 128 bytes apart
         const uint32_t ah = tc::smem_u32(Ahi), al = tc::smem_u32(Alo), bh = tc::smem_u32(Bhi),
                        bl = tc::smem_u32(Blo);
         for (int s = 0; s < Kp / 8; ++s) {
-            const uint64_t dah = tc::sdesc(ah + s * a_step, a_lbo, a_sbo);
-            const uint64_t dal = tc::sdesc(al + s * a_step, a_lbo, a_sbo);
-            const uint64_t dbh = tc::sdesc(bh + s * b_step, b_lbo, b_sbo);
-            const uint64_t dbl = tc::sdesc(bl + s * b_step, b_lbo, b_sbo);
-            tc::mma_tf32(tmem, dah, dbh, idesc, s > 0 ? 1u : 0u);
+            const uint32_t step = (uint32_t)s * 256u;
+            const uint64_t dah = tc::sdesc(ah + step, 128u, sbo);
+            const uint64_t dal = tc::sdesc(al + step, 128u, sbo);
+            const uint64_t dbh = tc::sdesc(bh + step, 128u, sbo);
+            const uint64_t dbl = tc::sdesc(bl + step, 128u, sbo);
+            tc::mma_tf32(tmem, dah, dbh, idesc, (s > 0 || terms == 2) ? 1u : 0u);
             if (terms == 3) {
                 tc::mma_tf32(tmem, dah, dbl, idesc, 1u);
                 tc::mma_tf32(tmem, dal, dbh, idesc, 1u);
@@ -90,7 +97,7 @@ __global__ void __launch_bounds__(kCheckThreads) k_tc_product(const float* __res
         }
         tc::mma_commit(&done);
     }
-    const bool ok = tc::mbar_wait(&done, 0);
+    const bool ok = terms == 0 || tc::mbar_wait(&done, 0);
     if (!ok && lane == 0) atomicOr(status, KERR_TIMEOUT);
     tc::fence_after_sync();
     if (warp < 4 && ok) {
@@ -121,13 +128,13 @@ extern "C" int fcw_tc_product_check(const float* a_dev, const float* b_dev, floa
                                     int32_t n, int32_t terms, int32_t trans, float* raw_dev, int32_t* status_dev,
                                     void* stream) {
     if (!a_dev || !b_dev || !c_dev || !status_dev) return FCW_E_INVALID;
-    if (m < 1 || m > 128 || k < 1 || k > 64 || (n != 64 && n != 128) || (terms != 1 && terms != 3) ||
+    if (m < 1 || m > 128 || k < 1 || k > 64 || (n != 64 && n != 128) || terms < 0 || terms > 3 ||
         (trans != 0 && trans != 1))
         return FCW_E_INVALID;
     const int MM = m <= 64 ? 64 : 128, Kp = (k + 7) / 8 * 8;
-    const size_t a_bytes = (size_t)(trans ? Kp : MM) * (trans ? MM : Kp) * 4;
+    const size_t a_bytes = (size_t)MM * Kp * 4;
     const size_t b_bytes = (size_t)Kp * n * 4;
-    const size_t smem = 2 * a_bytes + 2 * b_bytes + 4096;  // slack: an MN-major read runs past the last group
+    const size_t smem = 2 * a_bytes + 2 * b_bytes;
     cudaFuncSetAttribute(fcw::k_tc_product, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     fcw::k_tc_product<<<1, fcw::kCheckThreads, smem, static_cast<cudaStream_t>(stream)>>>(
         a_dev, b_dev, c_dev, m, k, n, terms, trans, raw_dev, status_dev);

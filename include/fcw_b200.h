@@ -223,7 +223,11 @@ int fcw_field_metrics_device(fcw_engine* e, const double* d_dev, const int32_t* 
  * or C = P^T B (trans = 1, P k x m row-major), B k x n row-major, C m x n, all
  * FP32 device arrays; m <= 128, k <= 64, n in {64, 128}. Each operand is split into
  * two TF32 terms and terms = 3 accumulates hi*hi + hi*lo + lo*hi (terms = 1: hi*hi)
- * with tcgen05.mma in tensor memory, through the sweeps' shared-memory layouts.
+ * with tcgen05.mma in tensor memory, through the sweeps' shared-memory layouts
+ * (both operands K-major; the transposed P is transposed as it is written, as the
+ * backward sweep's panels are).
+ * terms = 0 only writes lane l, column c of the accumulator as l * 1024 + c and
+ * reads it back (raw_dev); terms = 2 adds the hi*hi product to that pattern.
  * raw_dev (nullable) receives the 128 x n accumulator lanes; status_dev (one int,
  * zero on entry) gets a nonzero bit if the completion wait expired. */
 int fcw_tc_product_check(const float* a_dev, const float* b_dev, float* c_dev, int32_t m, int32_t k, int32_t n,
