@@ -626,7 +626,7 @@ def main(argv=None):
     ap.add_argument("--ref-sources-per-core", type=int, default=2)
     ap.add_argument("--quick", action="store_true", help="skip the FP64 forms and the accuracy check")
     ap.add_argument("--no-graphs", action="store_true", help="launch each block's kernels directly")
-    ap.add_argument("--tc-sweeps", type=int, default=1, choices=(0, 1),
+    ap.add_argument("--tc-sweeps", type=int, default=0, choices=(0, 1),
                     help="mixed Poisson sweeps on the tensor cores (1) or on FMA register tiles (0)")
     ap.add_argument("--autotune", action="store_true", help="choose block size and depth on the mesh first")
     ap.add_argument("--serving", action="store_true", help="run the serving stream instead (own JSON line)")

@@ -1020,7 +1020,7 @@ void fcw_default_params(fcw_params* p) {
     p->build_mixed = 1;
     p->device = 0;
     p->pipeline_depth = 4;
-    p->tc_sweeps = 1;
+    p->tc_sweeps = 0;
     p->robust = 0;
 }
 

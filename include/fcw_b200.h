@@ -49,7 +49,7 @@ typedef struct fcw_params {
     int32_t build_mixed;        /* also factor the grounded FP32 Poisson operator */
     int32_t device;             /* CUDA device ordinal */
     int32_t pipeline_depth;     /* blocks in flight on separate streams in the device metrics path (1-8) */
-    int32_t tc_sweeps;          /* mixed Poisson sweeps on the tensor cores (1, default) or FMA tiles (0) */
+    int32_t tc_sweeps;          /* mixed Poisson sweeps on the tensor cores (1) or FMA register tiles (0, default) */
     int32_t robust;             /* 1: operators of the intrinsic Delaunay triangulation (use_robust,
                                    distance_engines.py:119-125); 0 (default): the extrinsic cotan
                                    operators of fastcw_lean.py:394-413 */
@@ -98,7 +98,7 @@ enum {
 };
 
 /* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 64, mixed on, 4 blocks in flight,
- * tensor-core Poisson sweeps). */
+ * Poisson sweeps on FMA register tiles, extrinsic operators). */
 void fcw_default_params(fcw_params* p);
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between);

@@ -59,8 +59,7 @@ def test_corrupted_fields_are_flagged_and_neighbours_unaffected():
         # distance (core_analysis.py:1559-1564), the record keeps them for diagnosis
         assert np.all(np.isnan(r["radii"][j])) and np.all(np.isnan(r["perim"][j]))
         assert np.all(np.isnan(r["extra_r"][j])) and np.all(np.isnan(r["extra_a"][j]))
-    for j in (0, 2, 5):  # healthy neighbours in the same call: the records of the clean run
-        assert not r["bad"][j]
-        both = np.isnan(r["radii"][j]) & np.isnan(clean["radii"][j])
-        assert np.all(both | (r["radii"][j] == clean["radii"][j]))
-        assert r["msd_w"][j] == clean["msd_w"][j]
+    for j in (0, 2, 5):  # healthy neighbours in the same call: the records of the clean run (to the
+        assert not r["bad"][j]  # order of the band sums, which atomics set)
+        assert np.max(np.abs(r["radii"][j] - clean["radii"][j]) / clean["radii"][j]) <= 1e-12
+        assert abs(r["msd_w"][j] - clean["msd_w"][j]) <= 1e-12 * clean["msd_w"][j]

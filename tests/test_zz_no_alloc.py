@@ -98,8 +98,9 @@ def test_static_entry_first_on_a_fresh_engine_matches_the_reference_and_allocate
         with pytest.raises(_lib.FCWError) as ei:
             run(bad)
         assert ei.value.code == _lib.FCW_E_INVALID and "source index" in str(ei.value)
-        # the error word is cleared once reported: the next call succeeds
+        # the error word is cleared once reported: the next call succeeds (same records to the
+        # band-sum order, which atomics set)
         r2 = engine.split_records(run(), t.size, 3)
-        assert np.array_equal(r2["radii"], r["radii"], equal_nan=True)
+        assert np.max(np.abs(r2["radii"] - r["radii"]) / r["radii"]) <= 1e-12
     finally:
         eng.close()
