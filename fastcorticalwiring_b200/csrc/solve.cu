@@ -92,6 +92,22 @@ constexpr int depth_pad() { return sizeof(T) == 8 ? 4 : 1; }        // product d
 // f(row, col, T* v), v holding V adjacent columns.
 // ---------------------------------------------------------------------------
 
+// V adjacent elements (8 or 16 bytes, aligned) through L2 only: values other CTAs wrote.
+template <typename T, int V>
+__device__ __forceinline__ void ld_cg(const T* p, T* w) {
+    if constexpr (V * sizeof(T) == 16 && sizeof(T) == 4) {
+        const float4 x = __ldcg(reinterpret_cast<const float4*>(p));
+        w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+    } else if constexpr (V * sizeof(T) == 16) {
+        const double2 x = __ldcg(reinterpret_cast<const double2*>(p));
+        w[0] = x.x; w[1] = x.y;
+    } else {
+        static_assert(V == 2 && sizeof(T) == 4, "8-byte groups are float pairs");
+        const float2 x = __ldcg(reinterpret_cast<const float2*>(p));
+        w[0] = x.x; w[1] = x.y;
+    }
+}
+
 // Calls f(std::integral_constant<int, m>) with m = min(n, N), for n >= 1: the row
 // blocks a product needs, as a compile-time count.
 template <int N, class F>
@@ -538,13 +554,33 @@ __global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
         __syncthreads();
         if (!last_arrival) return;
         __threadfence();
+        // the partial sums in split order; four splits' vectors are loaded before any is added,
+        // so the loads overlap instead of waiting on one another
         acc.visit(ns, [&](int r, int c, T* v) {
+            constexpr int V = AccT::V;
+            const T* base = part + (int64_t)r * K + c;
+            const int64_t ss = (int64_t)PT * K;  // one split's slot
+            T sum[V];
 #pragma unroll
-            for (int q = 0; q < AccT::V; ++q) {
-                T sum = T(0);
-                for (int sp = 0; sp < nspl; ++sp) sum += __ldcg(&part[((int64_t)sp * PT + r) * K + c + q]);
-                v[q] = sum;
+            for (int q = 0; q < V; ++q) sum[q] = T(0);
+            int sp = 0;
+            for (; sp + 4 <= nspl; sp += 4) {
+                T w[4][V];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) ld_cg<T, V>(base + (sp + u) * ss, w[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int q = 0; q < V; ++q) sum[q] += w[u][q];
             }
+            for (; sp < nspl; ++sp) {
+                T w[V];
+                ld_cg<T, V>(base + sp * ss, w);
+#pragma unroll
+                for (int q = 0; q < V; ++q) sum[q] += w[q];
+            }
+#pragma unroll
+            for (int q = 0; q < V; ++q) v[q] = sum[q];
         });
         if (tid == 0) a.counters[(int64_t)s * a.ktiles + blockIdx.y] = 0;
     }
