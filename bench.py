@@ -42,18 +42,27 @@ METRIC = "sources/s @164k verts"
 N_BETWEEN = 3
 L2_BYTES = 126 * 1024 * 1024
 
-# DRAM bytes (read + write) per 1024-source block of each stage on the L7 mixed
-# workload, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum
-# summed over the stage's launches, divided by the 8 blocks of the process) of
-#   python bench.py --workload L7 --batch 1024 --steps 1 --warmup 3 --cpu-sample 0
-#       --quick --pipeline-depth 1
-# Other configurations report null.
-NCU_TRAFFIC = {
-    ("L7", 1024, "mixed"): {
-        "heat_fwd": 0.141e9, "heat_bwd": 2.725e9, "divergence": 2.097e9, "poisson_fwd": 2.941e9,
-        "poisson_bwd": 1.954e9, "shift": 1.329e9, "metrics": 1.773e9,
-    },
+# DRAM bytes (read + write) per 1024-source block of each stage, mixed precision, from one
+# ncu capture on the small L6 workload (36,866 cortical vertices; about 3.5 GB on the device):
+#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
+#       -c 90 -k 'regex:^k_(fwd|bwd|div_mixed|shift_stats|source_metrics|reach)$' --csv
+#       python bench.py --workload L6 --batch 1024 --steps 1 --warmup 3 --quick --cpu-sample 0 --pipeline-depth 1
+# (the first block's launches). Every stage moves n x K right-hand-side rows, so other meshes
+# report these bytes scaled by their vertex count (n / 36,866), labelled as scaled.
+TRAFFIC_L6_N = 36866
+TRAFFIC_L6 = {
+    "heat_fwd": 0.0720e9, "heat_bwd": 0.4775e9, "divergence": 0.4658e9, "poisson_fwd": 0.5230e9,
+    "poisson_bwd": 0.3583e9, "shift": 0.2889e9, "metrics": 0.4322e9,
 }
+
+
+def _traffic(stage, n, block_k, precision):
+    """(bytes, how) of a stage's DRAM traffic per block, or (None, None)."""
+    if block_k != 1024 or precision != "mixed" or stage not in TRAFFIC_L6:
+        return None, None
+    if n == TRAFFIC_L6_N:
+        return TRAFFIC_L6[stage], "ncu capture of this workload (L6)"
+    return TRAFFIC_L6[stage] * n / TRAFFIC_L6_N, f"L6 ncu capture scaled by n = {n} / {TRAFFIC_L6_N}"
 
 
 def _peaks():
@@ -428,9 +437,9 @@ def run_gpu(args):
             per_block_s = stages[dom] / 1e3
             byts = _stage_bytes(dom, pm.n_vertices, pm.n_faces, args.block_k, info["nnz_factor"], args.precision)
             ach = byts / per_block_s / 1e9
+            traffic, traffic_from = _traffic(dom, pm.n_vertices, args.block_k, args.precision)
             roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": hbm, "unit": "GB/s",
-                    "frac": ach / hbm,
-                    "traffic": NCU_TRAFFIC.get((args.workload, args.block_k, args.precision), {}).get(dom),
+                    "frac": ach / hbm, "traffic": traffic, "traffic_from": traffic_from,
                     "peak_kind": peak_kind,
                     "bytes_per_launch": byts, "launch": f"one {dom} stage on a {args.block_k}-source block"}
         line = {
