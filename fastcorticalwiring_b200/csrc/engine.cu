@@ -144,6 +144,30 @@ struct Workspace {
     }
 };
 
+// The single-source drop-in (fcw_compute_distance): the narrow panel layouts of the two FP64
+// factors, the task lists, its own vectors and sweep state, and its launch chain; built on
+// its first call.
+struct NarrowState {
+    bool ready = false;
+    fcw::NarrowLaunch L;
+    int64_t* at_ptr = nullptr;
+    double *at_h = nullptr, *at_p = nullptr;    // forward layouts of the heat and Poisson factors
+    double *atb_h = nullptr, *atb_p = nullptr;  // backward layouts
+    int4 *ftasks = nullptr, *btasks = nullptr;
+    int32_t n_ftasks = 0, n_btasks = 0;
+    double *u = nullptr, *div = nullptr, *y = nullptr, *out = nullptr;
+    double* pend = nullptr;       // entries a sweep's readers poll: heat and Poisson update entries, heat
+                                  // and Poisson solutions (set pending at the start of each call)
+    int* sync = nullptr;          // the four sweeps' ticket counters
+    // the heat forward's work list, built on the host per call: the source's elimination
+    // index, the path's task count, then (task, previous supernode on the path) pairs
+    int32_t* order = nullptr;
+    int32_t* horder = nullptr;    // pinned host staging of the list
+    std::vector<int32_t> fwd_first, nfwd_h;  // per supernode: first forward task, count
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;         // kernels per call
+};
+
 struct fcw_engine {
     fcw_params prm{};
     int device = 0;
@@ -205,6 +229,7 @@ struct fcw_engine {
     int64_t launches = 0;
     int32_t num_sms = 148;  // the device's multiprocessors (grid sizes of grid-stride kernels)
     int64_t n_flips = 0;    // intrinsic edge flips of the robust operators
+    NarrowState nar;
 
     // Device memory is stream-ordered (the device's default pool): freeing it
     // waits for this engine's streams only, never for other engines' work, so
@@ -259,6 +284,8 @@ struct fcw_engine {
             if (w.stream) cudaStreamDestroy(w.stream);
         }
         if (ev_in) cudaEventDestroy(ev_in);
+        if (nar.exec) cudaGraphExecDestroy(nar.exec);
+        if (nar.horder) cudaFreeHost(nar.horder);
         for (cudaEvent_t ev : event_pool) cudaEventDestroy(ev);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -1222,8 +1249,166 @@ int fcw_compute_distances(fcw_engine* e, const int32_t* sources, int64_t n, int3
     return FCW_OK;
 }
 
+namespace {
+
+// The drop-in's chain on st: the source's path, heat forward (the path's tasks) and
+// backward, divergence, Poisson forward and backward, shift into the caller's order.
+// Every sweep is one persistent ticketed launch. The source index is read from nar.src.
+int narrow_chain(fcw_engine* e, cudaStream_t st) {
+    NarrowState& q = e->nar;
+    const int64_t n = e->sym.n;
+    const int64_t nu = std::max<int64_t>(e->n_urows, 1);
+    double* U_h = q.pend;
+    double* U_p = q.pend + nu;
+    double* X_h = q.pend + 2 * nu;
+    double* X_p = X_h + n;
+    FCW_CUDA(cudaMemsetAsync(q.sync, 0, 4 * sizeof(int), st));
+    FCW_CUDA(cudaMemsetAsync(q.pend, 0xFF, (size_t)(2 * nu + 2 * n) * sizeof(double), st));  // pending
+    FCW_CUDA(cudaMemsetAsync(q.u, 0, (size_t)n * sizeof(double), st));
+    fcw::NarrowArgs a;
+    a.p = e->plan;
+    a.at_ptr = q.at_ptr;
+    a.uoff = e->uoff_d;
+    a.gm_ptr = e->gm_ptr_d;
+    a.gm_src = e->gm_src_d;
+    a.gm_child = e->gm_child_d;
+    a.iperm = e->iperm_d;
+    a.err = e->err_d;
+    // heat: the path's forward tasks, then the whole backward
+    mark(e, st, FCW_STAGE_HEAT_FWD);
+    a.at = q.at_h;
+    a.B = q.u;
+    a.U = U_h;
+    a.tasks = q.ftasks;
+    a.ntasks = q.n_ftasks;
+    a.order = q.order;
+    a.ticket = q.sync;
+    fcw::launch_fwd_narrow(a, true, q.L, st);
+    mark(e, st, FCW_STAGE_HEAT_BWD);
+    a.at = q.atb_h;
+    a.tasks = q.btasks;
+    a.ntasks = q.n_btasks;
+    a.X = X_h;
+    a.ticket = q.sync + 1;
+    fcw::launch_bwd_narrow(a, q.L, st);
+    mark(e, st, FCW_STAGE_DIVERGENCE);
+    fcw::launch_divergence_fp64_one(e->fd, X_h, q.div, st);
+    // Poisson (L + shift M)
+    mark(e, st, FCW_STAGE_POISSON_FWD);
+    a.at = q.at_p;
+    a.R = q.div;
+    a.B = q.y;
+    a.U = U_p;
+    a.tasks = q.ftasks;
+    a.ntasks = q.n_ftasks;
+    a.order = nullptr;
+    a.ticket = q.sync + 2;
+    fcw::launch_fwd_narrow(a, false, q.L, st);
+    mark(e, st, FCW_STAGE_POISSON_BWD);
+    a.at = q.atb_p;
+    a.tasks = q.btasks;
+    a.ntasks = q.n_btasks;
+    a.X = X_p;
+    a.ticket = q.sync + 3;
+    fcw::launch_bwd_narrow(a, q.L, st);
+    mark(e, st, FCW_STAGE_SHIFT);
+    fcw::launch_field_out_one((int32_t)n, X_p, q.order, e->iperm_d, q.out, e->num_sms, st);
+    mark(e, st, -1);
+    FCW_CUDA(cudaGetLastError());
+    return FCW_OK;
+}
+
+int narrow_ready(fcw_engine* e) {
+    NarrowState& q = e->nar;
+    if (q.ready) return FCW_OK;
+    const auto& S = e->sym;
+    const int32_t NS = S.nsuper;
+    const int64_t n = S.n;
+    if (fcw::configure_narrow_kernels(S.max_m, e->num_sms, &q.L) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(FCW_E_INVALID, "front too large for the single-source kernels (max_m " + std::to_string(S.max_m) +
+                                       ")");
+    }
+    std::vector<int64_t> ptr((size_t)NS + 1);
+    const int64_t total = fcw::narrow_layout(S.sn_c0.data(), S.sn_m.data(), NS, ptr.data());
+    std::vector<int4> ft, bt;
+    std::vector<int32_t> fptr, nf, nb;
+    fcw::narrow_tasks(S.sn_c0.data(), S.sn_m.data(), NS, S.level_nodes.data(), ft, fptr, nf, bt, nb);
+    q.n_ftasks = (int32_t)ft.size();
+    q.n_btasks = (int32_t)bt.size();
+    FCW_TRY(e->upload(&q.at_ptr, ptr));
+    FCW_TRY(e->upload(&q.ftasks, ft));
+    FCW_TRY(e->upload(&q.btasks, bt));
+    q.fwd_first = fptr;
+    q.nfwd_h = nf;
+    for (double** arr : {&q.at_h, &q.at_p, &q.atb_h, &q.atb_p}) {
+        FCW_TRY(e->dalloc(arr, (size_t)total));
+        FCW_CUDA(cudaMemsetAsync(*arr, 0, (size_t)total * sizeof(double), e->stream));
+    }
+    fcw::launch_build_narrow(e->plan, e->val_h, e->inv_h, q.at_ptr, q.at_h, q.atb_h, e->stream);
+    fcw::launch_build_narrow(e->plan, e->val_p, e->inv_p, q.at_ptr, q.at_p, q.atb_p, e->stream);
+    FCW_CUDA(cudaGetLastError());
+    FCW_TRY(e->dalloc(&q.u, (size_t)n));
+    FCW_TRY(e->dalloc(&q.div, (size_t)n));
+    FCW_TRY(e->dalloc(&q.y, (size_t)n));
+    FCW_TRY(e->dalloc(&q.out, (size_t)n));
+    FCW_TRY(e->dalloc(&q.pend, (size_t)(2 * std::max<int64_t>(e->n_urows, 1) + 2 * n)));
+    FCW_TRY(e->dalloc(&q.sync, 4));
+    const size_t cap = 2 + 2 * (size_t)q.n_ftasks;
+    FCW_TRY(e->dalloc(&q.order, cap));
+    FCW_CUDA(cudaHostAlloc(&q.horder, cap * sizeof(int32_t), cudaHostAllocDefault));
+    FCW_CUDA(cudaStreamSynchronize(e->stream));
+    q.launches = 6;
+    if (e->graphs_on) {
+        FCW_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        const int lrc = narrow_chain(e, e->stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+        if (lrc != FCW_OK) {
+            if (g) cudaGraphDestroy(g);
+            return lrc;
+        }
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&q.exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {  // not capturable here: the chain launches directly
+            cudaGetLastError();
+            q.exec = nullptr;
+        }
+    }
+    q.ready = true;
+    return FCW_OK;
+}
+
+}  // namespace
+
 int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host) {
-    return fcw_compute_distances(e, &source, 1, FCW_PREC_FP64, out_host);
+    FCW_TRY(check_engine(e));
+    if (!out_host) return fail(FCW_E_INVALID, "NULL argument");
+    if (source < 0 || source >= e->sym.n)
+        return fail(FCW_E_INVALID, "source_idx out of range: " + std::to_string(source) + " for mesh with " +
+                                       std::to_string(e->sym.n) + " vertices");
+    FCW_TRY(narrow_ready(e));
+    NarrowState& q = e->nar;
+    cudaStream_t st = e->stream;
+    // the source's path to the root, bottom-up, with each supernode's forward tasks
+    const auto& S = e->sym;
+    int32_t* o = q.horder;
+    int32_t len = 0, prev = -1;
+    o[0] = S.iperm[source];
+    for (int32_t s = S.col_sn[o[0]]; s >= 0; prev = s, s = S.sn_parent[s])
+        for (int32_t t = q.fwd_first[s]; t < q.fwd_first[s] + q.nfwd_h[s]; ++t) {
+            o[2 + 2 * len] = t;
+            o[3 + 2 * len] = prev;
+            ++len;
+        }
+    o[1] = len;
+    FCW_CUDA(cudaMemcpyAsync(q.order, o, (size_t)(2 + 2 * len) * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    if (q.exec && e->graphs_on && !e->prof_on) FCW_CUDA(cudaGraphLaunch(q.exec, st));
+    else FCW_TRY(narrow_chain(e, st));
+    e->launches += q.launches;
+    FCW_CUDA(cudaMemcpyAsync(out_host, q.out, (size_t)e->sym.n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FCW_CUDA(cudaStreamSynchronize(st));
+    return check_kernel_errors(e, "distance");
 }
 
 namespace {

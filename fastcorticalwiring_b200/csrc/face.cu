@@ -26,12 +26,9 @@ __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, 
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 
-__global__ void __launch_bounds__(256) k_div_fp64(FaceData fd, const double* __restrict__ u,
-                                                  double* __restrict__ div, int32_t K) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int v = blockIdx.x * 8 + warp;
-    if (v >= fd.nv) return;
-    const int col = blockIdx.y * kSlice + lane;
+// The divergence at vertex v of column col of u (leading dimension K).
+__device__ __forceinline__ double div_at(const FaceData& fd, const double* __restrict__ u, int64_t K, int64_t col,
+                                         int v) {
     double acc = 0.0;
     for (int q = fd.inc_ptr[v]; q < fd.inc_ptr[v + 1]; ++q) {
         const int f = fd.inc_face[q];
@@ -50,7 +47,23 @@ __global__ void __launch_bounds__(256) k_div_fp64(FaceData fd, const double* __r
         const double* b = g + 3 * c;
         acc = add(acc, mul(s, add(add(mul(gx, b[0]), mul(gy, b[1])), mul(gz, b[2]))));
     }
-    div[(int64_t)v * K + col] = acc;
+    return acc;
+}
+
+__global__ void __launch_bounds__(256) k_div_fp64(FaceData fd, const double* __restrict__ u,
+                                                  double* __restrict__ div, int32_t K) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int v = blockIdx.x * 8 + warp;
+    if (v >= fd.nv) return;
+    const int col = blockIdx.y * kSlice + lane;
+    div[(int64_t)v * K + col] = div_at(fd, u, K, col, v);
+}
+
+// One column: a thread per vertex.
+__global__ void __launch_bounds__(256) k_div_fp64_one(FaceData fd, const double* __restrict__ u,
+                                                      double* __restrict__ div) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < fd.nv) div[v] = div_at(fd, u, 1, 0, v);
 }
 
 // 2^-e for the binary exponent e of |x| (x normal, nonzero): exact scaling to [1, 2).
@@ -134,6 +147,10 @@ __global__ void __launch_bounds__(256) k_div_mixed(FaceData fd, const double* __
 void launch_divergence_fp64(const FaceData& fd, const double* u, double* div, int32_t K, cudaStream_t st) {
     if (fd.nv <= 0 || K <= 0) return;
     k_div_fp64<<<dim3((fd.nv + 7) / 8, K / kSlice), 256, 0, st>>>(fd, u, div, K);
+}
+
+void launch_divergence_fp64_one(const FaceData& fd, const double* u, double* div, cudaStream_t st) {
+    if (fd.nv > 0) k_div_fp64_one<<<(fd.nv + 255) / 256, 256, 0, st>>>(fd, u, div);
 }
 
 void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace fcw {
 
 // Error bits a kernel may raise (OR-ed into a device word read by the host).
@@ -123,6 +125,53 @@ int make_rows_map(CUtensorMap* map, const float* base, int64_t n, int32_t K);
 void launch_build_cores(const DevPlan& p, const double* val, const double* inv, const int64_t* core_ptr,
                         float* hi, float* lo, float* hiT, float* loT, cudaStream_t st);
 
+// ---- one right-hand side: the single-source drop-in (solve_narrow.cu) ----
+constexpr int kNarrowRows = 64;            // stacked rows per chunk of the narrow layout
+constexpr int kNarrowTaskDoubles = 12288;  // panel data of one task (96 KB); fronts up to this many rows
+struct NarrowArgs {
+    DevPlan p;
+    const double* at = nullptr;       // per supernode [inv(L_ss); Q_s]: forward, 64-row column-major chunks;
+                                      // backward, column-major over all rows
+    const int64_t* at_ptr = nullptr;  // per supernode: offset (doubles, even) in either layout
+    const int4* tasks = nullptr;      // forward: (s, first chunk, chunks); backward: (s, j0, j1)
+    int32_t ntasks = 0;
+    // heat forward: the source's elimination index, the path's task count, then (task,
+    // previous supernode on the path) pairs bottom-up
+    const int32_t* order = nullptr;
+    const double* R = nullptr;        // forward right-hand side (n)
+    double* B = nullptr;              // forward result (n)
+    double* X = nullptr;              // backward: the solution (n), pending on entry
+    double* U = nullptr;              // forward update entries (sum nr), pending on entry
+    const int64_t* uoff = nullptr;
+    const int32_t* gm_ptr = nullptr;
+    const int32_t* gm_src = nullptr;
+    const int32_t* gm_child = nullptr;
+    int* ticket = nullptr;            // zero when a sweep starts
+    const int32_t* iperm = nullptr;
+    int* err = nullptr;
+};
+struct NarrowLaunch {
+    int grid_fwd = 0, grid_bwd = 0;
+    size_t fwd_smem = 0, bwd_smem = 0;
+};
+// Chunk offsets of the narrow layout (nsuper + 1 entries); returns the doubles it holds.
+int64_t narrow_layout(const int32_t* sn_c0, const int32_t* sn_m, int32_t nsuper, int64_t* at_ptr);
+// Forward tasks in level order (supernode s's are the nfwd[s] from fwd_first[s]), backward
+// tasks in reversed level order, and each supernode's task counts.
+void narrow_tasks(const int32_t* sn_c0, const int32_t* sn_m, int32_t nsuper, const int32_t* level_nodes,
+                  std::vector<int4>& fwd, std::vector<int32_t>& fwd_first, std::vector<int32_t>& nfwd,
+                  std::vector<int4>& bwd, std::vector<int32_t>& nbwd);
+void launch_build_narrow(const DevPlan& p, const double* val, const double* inv, const int64_t* at_ptr,
+                         double* at_f, double* at_b, cudaStream_t st);
+cudaError_t configure_narrow_kernels(int max_m, int num_sms, NarrowLaunch* L);
+// Forward sweep (delta: the identity column of a.order's source over its path's tasks; B
+// zero on entry), backward sweep.
+void launch_fwd_narrow(const NarrowArgs& a, bool delta, const NarrowLaunch& L, cudaStream_t st);
+void launch_bwd_narrow(const NarrowArgs& a, const NarrowLaunch& L, cudaStream_t st);
+// out[i] = Y[iperm[i]] - Y[*src_elim] (caller's order, shifted to zero at the source)
+void launch_field_out_one(int32_t n, const double* Y, const int32_t* src_elim, const int32_t* iperm, double* out,
+                          int num_sms, cudaStream_t st);
+
 // ---- fused gradient -> normalise -> divergence (face.cu) ----
 struct FaceData {
     int32_t nv = 0, nf = 0;
@@ -141,6 +190,8 @@ struct FaceData {
     const float2* inc_w = nullptr;
 };
 void launch_divergence_fp64(const FaceData& fd, const double* u, double* div, int32_t K, cudaStream_t st);
+// One column (K = 1), the same arithmetic per vertex.
+void launch_divergence_fp64_one(const FaceData& fd, const double* u, double* div, cudaStream_t st);
 void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,
                              cudaStream_t st);
 
