@@ -1283,14 +1283,14 @@ int narrow_chain(fcw_engine* e, cudaStream_t st) {
     a.ntasks = q.n_ftasks;
     a.order = q.order;
     a.ticket = q.sync;
-    fcw::launch_fwd_narrow(a, true, q.L, st);
+    fcw::launch_fwd_narrow(a, true, false, q.L, st);
     mark(e, st, FCW_STAGE_HEAT_BWD);
     a.at = q.atb_h;
     a.tasks = q.btasks;
     a.ntasks = q.n_btasks;
     a.X = X_h;
     a.ticket = q.sync + 1;
-    fcw::launch_bwd_narrow(a, q.L, st);
+    fcw::launch_bwd_narrow(a, !e->prof_on, q.L, st);
     mark(e, st, FCW_STAGE_DIVERGENCE);
     fcw::launch_divergence_fp64_one(e->fd, X_h, q.div, st);
     // Poisson (L + shift M)
@@ -1303,14 +1303,14 @@ int narrow_chain(fcw_engine* e, cudaStream_t st) {
     a.ntasks = q.n_ftasks;
     a.order = nullptr;
     a.ticket = q.sync + 2;
-    fcw::launch_fwd_narrow(a, false, q.L, st);
+    fcw::launch_fwd_narrow(a, false, !e->prof_on, q.L, st);
     mark(e, st, FCW_STAGE_POISSON_BWD);
     a.at = q.atb_p;
     a.tasks = q.btasks;
     a.ntasks = q.n_btasks;
     a.X = X_p;
     a.ticket = q.sync + 3;
-    fcw::launch_bwd_narrow(a, q.L, st);
+    fcw::launch_bwd_narrow(a, !e->prof_on, q.L, st);
     mark(e, st, FCW_STAGE_SHIFT);
     fcw::launch_field_out_one((int32_t)n, X_p, q.order, e->iperm_d, q.out, e->num_sms, st);
     mark(e, st, -1);

@@ -26,26 +26,35 @@ __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, 
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 
-// The divergence at vertex v of column col of u (leading dimension K).
+// The term of incidence q (a face of vertex v, at corner c) in column col of u (leading
+// dimension K); false when the face's gradient vanishes (the face is skipped).
+__device__ __forceinline__ bool face_term(const FaceData& fd, const double* __restrict__ u, int64_t K, int64_t col,
+                                          int q, double& t) {
+    const int f = fd.inc_face[q];
+    const int c = fd.inc_corner[q];
+    const int i0 = fd.fv[3 * f], i1 = fd.fv[3 * f + 1], i2 = fd.fv[3 * f + 2];
+    const double* g = fd.gb + 9 * (int64_t)f;
+    const double u0 = u[(int64_t)i0 * K + col];
+    const double du1 = sub(u[(int64_t)i1 * K + col], u0);
+    const double du2 = sub(u[(int64_t)i2 * K + col], u0);
+    const double gx = add(mul(du1, g[3]), mul(du2, g[6]));
+    const double gy = add(mul(du1, g[4]), mul(du2, g[7]));
+    const double gz = add(mul(du1, g[5]), mul(du2, g[8]));
+    const double nn = __dsqrt_rn(add(add(mul(gx, gx), mul(gy, gy)), mul(gz, gz)));
+    if (!(nn > 1e-300)) return false;
+    const double s = __ddiv_rn(-fd.garea[f], nn);
+    const double* b = g + 3 * c;
+    t = mul(s, add(add(mul(gx, b[0]), mul(gy, b[1])), mul(gz, b[2])));
+    return true;
+}
+
+// The divergence at vertex v of column col of u: its faces' terms in incidence order.
 __device__ __forceinline__ double div_at(const FaceData& fd, const double* __restrict__ u, int64_t K, int64_t col,
                                          int v) {
     double acc = 0.0;
     for (int q = fd.inc_ptr[v]; q < fd.inc_ptr[v + 1]; ++q) {
-        const int f = fd.inc_face[q];
-        const int c = fd.inc_corner[q];
-        const int i0 = fd.fv[3 * f], i1 = fd.fv[3 * f + 1], i2 = fd.fv[3 * f + 2];
-        const double* g = fd.gb + 9 * (int64_t)f;
-        const double u0 = u[(int64_t)i0 * K + col];
-        const double du1 = sub(u[(int64_t)i1 * K + col], u0);
-        const double du2 = sub(u[(int64_t)i2 * K + col], u0);
-        const double gx = add(mul(du1, g[3]), mul(du2, g[6]));
-        const double gy = add(mul(du1, g[4]), mul(du2, g[7]));
-        const double gz = add(mul(du1, g[5]), mul(du2, g[8]));
-        const double nn = __dsqrt_rn(add(add(mul(gx, gx), mul(gy, gy)), mul(gz, gz)));
-        if (!(nn > 1e-300)) continue;
-        const double s = __ddiv_rn(-fd.garea[f], nn);
-        const double* b = g + 3 * c;
-        acc = add(acc, mul(s, add(add(mul(gx, b[0]), mul(gy, b[1])), mul(gz, b[2]))));
+        double t;
+        if (face_term(fd, u, K, col, q, t)) acc = add(acc, t);
     }
     return acc;
 }
@@ -59,9 +68,10 @@ __global__ void __launch_bounds__(256) k_div_fp64(FaceData fd, const double* __r
     div[(int64_t)v * K + col] = div_at(fd, u, K, col, v);
 }
 
-// One column: a thread per vertex.
+// One column: a thread per vertex (its face loop's loads are independent, so they overlap).
 __global__ void __launch_bounds__(256) k_div_fp64_one(FaceData fd, const double* __restrict__ u,
                                                       double* __restrict__ div) {
+    asm volatile("griddepcontrol.launch_dependents;");
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < fd.nv) div[v] = div_at(fd, u, 1, 0, v);
 }

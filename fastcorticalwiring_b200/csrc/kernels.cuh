@@ -166,8 +166,10 @@ void launch_build_narrow(const DevPlan& p, const double* val, const double* inv,
 cudaError_t configure_narrow_kernels(int max_m, int num_sms, NarrowLaunch* L);
 // Forward sweep (delta: the identity column of a.order's source over its path's tasks; B
 // zero on entry), backward sweep.
-void launch_fwd_narrow(const NarrowArgs& a, bool delta, const NarrowLaunch& L, cudaStream_t st);
-void launch_bwd_narrow(const NarrowArgs& a, const NarrowLaunch& L, cudaStream_t st);
+// overlap: start while the stream's previous kernel finishes (programmatic dependent launch);
+// that kernel's results are read only once it has completed.
+void launch_fwd_narrow(const NarrowArgs& a, bool delta, bool overlap, const NarrowLaunch& L, cudaStream_t st);
+void launch_bwd_narrow(const NarrowArgs& a, bool overlap, const NarrowLaunch& L, cudaStream_t st);
 // out[i] = Y[iperm[i]] - Y[*src_elim] (caller's order, shifted to zero at the source)
 void launch_field_out_one(int32_t n, const double* Y, const int32_t* src_elim, const int32_t* iperm, double* out,
                           int num_sms, cudaStream_t st);

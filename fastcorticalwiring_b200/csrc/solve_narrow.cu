@@ -116,6 +116,12 @@ __device__ __forceinline__ void wait_copies(uint64_t* bar, uint32_t parity, int*
     }
 }
 
+// Programmatic dependent launch: the next kernel of the stream may start (its CTAs take
+// tickets and start their panel copies, which read nothing this kernel writes) while this
+// one finishes; it reads this kernel's results only after griddepcontrol.wait.
+__device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void wait_predecessor() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __host__ __device__ __forceinline__ int chunk_rows(int m, int c) { return min(CR, m - CR * c); }
 __host__ __device__ __forceinline__ int even(int x) { return (x + 1) & ~1; }
 
@@ -223,6 +229,7 @@ __global__ void __launch_bounds__(NTN, 2) k_fwd_tasks(NarrowArgs a) {
     __shared__ int task, task_prev;
     const int tid = threadIdx.x;
     const DevPlan& p = a.p;
+    allow_dependents();
     if (tid == 0) {
         tc::mbar_init(&bar, 1);
         tc::fence_mbar_init();
@@ -231,6 +238,7 @@ __global__ void __launch_bounds__(NTN, 2) k_fwd_tasks(NarrowArgs a) {
     const int total = DELTA ? a.order[1] : a.ntasks;
     const int se = DELTA ? a.order[0] : -1;
     uint32_t parity = 0;
+    bool inputs_ready = false;  // the previous kernel's results (right-hand side) are visible
     for (;;) {
         if (tid == 0) {
             const int t = atomicAdd(a.ticket, 1);
@@ -253,6 +261,10 @@ __global__ void __launch_bounds__(NTN, 2) k_fwd_tasks(NarrowArgs a) {
             for (int k = 0; k < nc; ++k)
                 tc::bulk_load(dat + k * kChunk, a.at + a.at_ptr[s] + (int64_t)(cb + k) * CR * ns,
                               (uint32_t)(ns * even(chunk_rows(m, cb + k))) * 8u, &bar);
+        }
+        if (!inputs_ready) {
+            wait_predecessor();
+            inputs_ready = true;
         }
         // thread t < 64: column row t (W); thread 64 + i: structure row Rs + i of the task
         const int row = tid < kMaxWidth ? (tid < ns ? tid : -1)
@@ -292,12 +304,14 @@ __global__ void __launch_bounds__(NTN, 2) k_bwd_tasks(NarrowArgs a) {
     __shared__ int task;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const DevPlan& p = a.p;
+    allow_dependents();
     if (tid == 0) {
         tc::mbar_init(&bar, 1);
         tc::fence_mbar_init();
     }
     __syncthreads();
     uint32_t parity = 0;
+    bool inputs_ready = false;  // the previous kernel's results (forward result) are visible
     for (;;) {
         if (tid == 0) {
             const int t = atomicAdd(a.ticket, 1);
@@ -314,6 +328,10 @@ __global__ void __launch_bounds__(NTN, 2) k_bwd_tasks(NarrowArgs a) {
             const uint32_t bytes = (uint32_t)(nj * mp) * 8u;
             tc::mbar_arrive_expect_tx(&bar, bytes);
             tc::bulk_load(dat, a.at + a.at_ptr[s] + (int64_t)j0 * mp, bytes, &bar);
+        }
+        if (!inputs_ready) {
+            wait_predecessor();
+            inputs_ready = true;
         }
         // The parent's columns come first among the structure rows (its first column is the
         // smallest structure row) and are written last, just before this task can run: warp 0
@@ -434,12 +452,30 @@ cudaError_t configure_narrow_kernels(int max_m, int num_sms, NarrowLaunch* L) {
     return e;
 }
 
-void launch_fwd_narrow(const NarrowArgs& a, bool delta, const NarrowLaunch& L, cudaStream_t st) {
-    if (delta) k_fwd_tasks<true><<<L.grid_fwd, NTN, L.fwd_smem, st>>>(a);
-    else k_fwd_tasks<false><<<L.grid_fwd, NTN, L.fwd_smem, st>>>(a);
+namespace {
+// overlap: launched as a programmatic dependent of the stream's previous kernel
+template <typename Kern>
+void launch_sweep(Kern kern, int grid, size_t smem, bool overlap, const NarrowArgs& a, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(NTN);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = overlap ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kern, a);
 }
-void launch_bwd_narrow(const NarrowArgs& a, const NarrowLaunch& L, cudaStream_t st) {
-    k_bwd_tasks<<<L.grid_bwd, NTN, L.bwd_smem, st>>>(a);
+}  // namespace
+
+void launch_fwd_narrow(const NarrowArgs& a, bool delta, bool overlap, const NarrowLaunch& L, cudaStream_t st) {
+    if (delta) launch_sweep(k_fwd_tasks<true>, L.grid_fwd, L.fwd_smem, overlap, a, st);
+    else launch_sweep(k_fwd_tasks<false>, L.grid_fwd, L.fwd_smem, overlap, a, st);
+}
+void launch_bwd_narrow(const NarrowArgs& a, bool overlap, const NarrowLaunch& L, cudaStream_t st) {
+    launch_sweep(k_bwd_tasks, L.grid_bwd, L.bwd_smem, overlap, a, st);
 }
 void launch_field_out_one(int32_t n, const double* Y, const int32_t* src_elim, const int32_t* iperm, double* out,
                           int num_sms, cudaStream_t st) {

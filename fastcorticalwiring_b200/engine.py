@@ -31,6 +31,30 @@ ENGINE_DEFAULTS = dict(block_k=1024, leaf_size=64, max_width=64, relax=64, build
                        tc_sweeps=0, robust=0)
 
 
+_PINNED = None
+
+
+def _field_array(n: int) -> np.ndarray:
+    """A new float64 array for one field, in page-locked host memory when CUDA is up, so the
+    device copies into it at full speed (about 3x a copy into pageable memory, which the
+    driver stages through a bounce buffer). The memory comes from torch's caching host
+    allocator, which takes the block back when the array is freed and hands it out again,
+    so a loop of single-source calls allocates nothing after its first calls."""
+    global _PINNED
+    if _PINNED is None:
+        try:
+            import torch
+
+            _PINNED = bool(torch.cuda.is_available())
+        except Exception:
+            _PINNED = False
+    if _PINNED:
+        import torch
+
+        return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    return np.empty(n, dtype=np.float64)
+
+
 class HeatEngine:
     """One cortical submesh factored on one GPU."""
 
@@ -76,7 +100,7 @@ class HeatEngine:
 
     # -- distances -------------------------------------------------------
     def compute_distance(self, source_idx: int) -> np.ndarray:
-        out = np.empty(self.n_vertices, dtype=np.float64)
+        out = _field_array(self.n_vertices)
         _lib.check(_lib.load().fcw_compute_distance(self.handle, int(source_idx), _lib.ptr(out)))
         return out
 
