@@ -288,8 +288,11 @@ def _stage_bytes(stage, n, nf, K, nnz_factor, precision, nreached_rows=None):
 
 
 def shard_sources(order, world, rank):
-    """Rank `rank`'s contiguous slice of the BFS order: every source on exactly one rank."""
-    return np.array_split(np.asarray(order), world)[rank]
+    """Rank `rank`'s contiguous slice of the BFS order: every source on exactly one rank (the
+    product's sharding, fastcorticalwiring_b200.sharded)."""
+    from fastcorticalwiring_b200 import sharded
+
+    return sharded.shard(order, world, rank)
 
 
 def max_over_ranks(x, dist, device):

@@ -45,6 +45,7 @@ class FCWParams(ctypes.Structure):
         ("pipeline_depth", ctypes.c_int32),
         ("tc_sweeps", ctypes.c_int32),
         ("robust", ctypes.c_int32),
+        ("refine", ctypes.c_int32),
     ]
 
 

@@ -192,6 +192,7 @@ struct fcw_engine {
     int64_t n_urows = 0, n_parts = 0;
     double *val_h = nullptr, *inv_h = nullptr, *val_p = nullptr, *inv_p = nullptr;
     float *val_g = nullptr, *inv_g = nullptr;
+    fcw::CsrOperator lg;  // the grounded Poisson operator in FP64, elimination order (refinement residuals)
     // tensor-core FP32 sweeps: core arrays of the grounded factor and the forward task list
     float *core_hi = nullptr, *core_lo = nullptr, *coreT_hi = nullptr, *coreT_lo = nullptr;
     int64_t* core_ptr_d = nullptr;
@@ -357,6 +358,7 @@ int validate_params(const fcw_params* p) {
     if (p->pipeline_depth < 1 || p->pipeline_depth > 8) return fail(FCW_E_INVALID, "pipeline_depth must be in [1, 8]");
     if (p->tc_sweeps != 0 && p->tc_sweeps != 1) return fail(FCW_E_INVALID, "tc_sweeps must be 0 or 1");
     if (p->robust != 0 && p->robust != 1) return fail(FCW_E_INVALID, "robust must be 0 or 1");
+    if (p->refine < 0 || p->refine > 4) return fail(FCW_E_INVALID, "refine must be in [0, 4]");
     return FCW_OK;
 }
 
@@ -671,6 +673,37 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     };
     FCW_TRY(run_factor(Op::Heat, e->val_h, e->inv_h, "heat factorisation"));
     FCW_TRY(run_factor(Op::Poisson, e->val_p, e->inv_p, "Poisson factorisation"));
+    if (e->prm.build_mixed && e->prm.refine > 0) {
+        // L_g in CSR, elimination order: the entries the FP32 factor came from
+        const int32_t gold = S.perm[e->ground_new];
+        std::vector<int64_t> rp(S.n + 1, 0);
+        std::vector<int32_t> ci;
+        std::vector<double> av;
+        ci.reserve(m.Li.size());
+        av.reserve(m.Li.size());
+        for (int64_t i = 0; i < S.n; ++i) {
+            const int32_t old = S.perm[i];
+            for (int64_t k = m.Lp[old]; k < m.Lp[old + 1]; ++k) {
+                const int32_t j = m.Li[k];
+                const bool diag = j == old;
+                const double v = (old == gold || j == gold) ? (diag ? 1.0 : 0.0) : m.Lx[k];
+                if (v == 0.0 && !diag) continue;
+                ci.push_back(S.iperm[j]);
+                av.push_back(v);
+            }
+            rp[i + 1] = (int64_t)ci.size();
+        }
+        int64_t* rp_d;
+        int32_t* ci_d;
+        double* av_d;
+        FCW_TRY(e->upload(&rp_d, rp));
+        FCW_TRY(e->upload(&ci_d, ci));
+        FCW_TRY(e->upload(&av_d, av));
+        e->lg.n = (int32_t)S.n;
+        e->lg.rp = rp_d;
+        e->lg.ci = ci_d;
+        e->lg.av = av_d;
+    }
     if (e->prm.build_mixed) {
         double *val_tmp, *inv_tmp;
         FCW_TRY(e->dalloc(&val_tmp, S.nnz_factor));
@@ -872,6 +905,16 @@ int distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, co
         float* Y = reinterpret_cast<float*>(w.Y);
         fcw::launch_divergence_mixed(e->fd, w.Bh, w.Bp32, K, e->ground_new, st);
         FCW_TRY(poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, Y, K, st));
+        // refinement: residual in FP64 and its FP32 solution, in the shift's output buffer
+        // (two n x K float halves of dT64) before the shift writes it
+        for (int32_t it = 0; it < e->prm.refine && e->lg.rp; ++it) {
+            float* r = w.dT32;
+            float* d = w.dT32 + (int64_t)n * K;
+            fcw::launch_residual(e->lg, K, w.Bp32, Y, r, st);
+            FCW_TRY(poisson_solve<float>(e, e->val_g, e->inv_g, r, d, K, st));
+            fcw::launch_add((int64_t)n * K, Y, d, e->num_sms, st);
+            e->launches += 2;
+        }
         mark(e, st, FCW_STAGE_SHIFT);
         if (ma) fcw::launch_shift_stats<float, float>(*ma, K, Y, w.dT32, st);
         else fcw::launch_shift_transpose<float, float>(n, K, Y, w.src, w.dT32, st);
@@ -1049,6 +1092,7 @@ void fcw_default_params(fcw_params* p) {
     p->pipeline_depth = 4;
     p->tc_sweeps = 0;
     p->robust = 0;
+    p->refine = 0;
 }
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between) {

@@ -174,6 +174,18 @@ void launch_bwd_narrow(const NarrowArgs& a, bool overlap, const NarrowLaunch& L,
 void launch_field_out_one(int32_t n, const double* Y, const int32_t* src_elim, const int32_t* iperm, double* out,
                           int num_sms, cudaStream_t st);
 
+// ---- iterative refinement of the mixed Poisson solve (refine.cu) ----
+struct CsrOperator {
+    int32_t n = 0;
+    const int64_t* rp = nullptr;  // n + 1
+    const int32_t* ci = nullptr;
+    const double* av = nullptr;
+};
+// r = b - A x (n x K row-major FP32 blocks, K a multiple of 4), accumulated in FP64
+void launch_residual(const CsrOperator& A, int32_t K, const float* b, const float* x, float* r, cudaStream_t st);
+// y += d over count floats (a multiple of 4)
+void launch_add(int64_t count, float* y, const float* d, int num_sms, cudaStream_t st);
+
 // ---- fused gradient -> normalise -> divergence (face.cu) ----
 struct FaceData {
     int32_t nv = 0, nf = 0;

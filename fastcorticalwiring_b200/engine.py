@@ -28,7 +28,7 @@ MIN_DIFFUSION_LENGTH_MM = 0.5              # distance_engines.py:13
 RECOMMENDED_MIN_DIFFUSION_LENGTH_MM = 0.7  # distance_engines.py:14
 
 ENGINE_DEFAULTS = dict(block_k=1024, leaf_size=64, max_width=64, relax=64, build_mixed=1, device=0, pipeline_depth=4,
-                       tc_sweeps=0, robust=0)
+                       tc_sweeps=0, robust=0, refine=0)
 
 
 _PINNED = None

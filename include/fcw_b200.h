@@ -53,6 +53,9 @@ typedef struct fcw_params {
     int32_t robust;             /* 1: operators of the intrinsic Delaunay triangulation (use_robust,
                                    distance_engines.py:119-125); 0 (default): the extrinsic cotan
                                    operators of fastcw_lean.py:394-413 */
+    int32_t refine;             /* mixed form: iterative-refinement steps of the FP32 Poisson solve
+                                   (0-4, default 0): each computes the residual of the grounded
+                                   system in FP64 and adds the FP32 solution of it */
 } fcw_params;
 
 typedef struct fcw_info {
@@ -98,7 +101,7 @@ enum {
 };
 
 /* Fill *p with the defaults (0.7 mm, 1e-10, K=1024, leaf 64, width 64, relax 64, mixed on, 4 blocks in flight,
- * Poisson sweeps on FMA register tiles, extrinsic operators). */
+ * Poisson sweeps on FMA register tiles, extrinsic operators, no refinement). */
 void fcw_default_params(fcw_params* p);
 
 int fcw_metrics_stride(int32_t n_targets, int32_t n_between);

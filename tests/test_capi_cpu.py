@@ -157,3 +157,16 @@ def test_registered_engine_subclasses_the_host_contract():
     z, pm = _l4()
     with pytest.raises(_lib.FCWError):  # no device here: construction reaches the engine and fails loudly
         cls(pm.V, pm.F)
+
+
+def test_refine_steps_are_validated():
+    """fcw_params.refine (iterative-refinement steps of the mixed Poisson solve) is checked on
+    the host: 0-4 are accepted, other values are FCW_E_INVALID."""
+    from fastcorticalwiring_b200 import _lib
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    m = folded_icosphere(2, seed=0, jitter=0.0)
+    _lib.analyze(m.vertices, m.faces, refine=2)
+    for bad in (-1, 5):
+        with pytest.raises(_lib.FCWError):
+            _lib.analyze(m.vertices, m.faces, refine=bad)

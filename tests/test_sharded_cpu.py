@@ -1,0 +1,132 @@
+"""ShardedWiringAnalysis on two gloo ranks (CPU): each rank computes the records of its slice
+of the BFS sources, the records are gathered in rank order, and both ranks end with arrays
+identical to a one-process run on the same records.
+
+The engine is replaced by a stand-in whose records and samples are functions of the source
+index (the sharding and the gather are under test here, not the solver, which the GPU tests
+cover); it also reports which sources each rank computed."""
+import datetime
+import multiprocessing as mp
+import os
+import socket
+
+import numpy as np
+
+from fastcorticalwiring_b200 import _lib
+from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+SCALES = (0.001, 0.004, 0.016)
+
+
+class _StandInEngine:
+    def __init__(self):
+        self.seen = []
+
+    def compute_metrics(self, sources, targets, n_between=3, eps=1e-6, precision="mixed"):
+        src = np.asarray(sources, dtype=np.float64)
+        self.seen.extend(np.asarray(sources).tolist())
+        nt = len(targets)
+        rec = np.zeros((src.size, _lib.metrics_stride(nt, n_between)))
+        rec[:, 0], rec[:, 1], rec[:, 2] = src * 0.5, src * 0.25, src + 1.0
+        rec[:, 5] = (np.asarray(sources) % 17 == 0).astype(float)  # some flagged fields
+        for i in range(nt):
+            rec[:, 7 + i] = src + i
+            rec[:, 7 + nt + i] = 2.0 * src + i
+        return rec
+
+    def assemble_samples(self, records, targets, n_between=3, boundary_cap=None):
+        n = records.shape[0]
+        cap = _lib.samples_capacity(len(targets), n_between)
+        counts = (records[:, 2].astype(np.int64) % 5).astype(np.int32)
+        radii = np.tile(np.arange(cap, dtype=np.float32), (n, 1)) + records[:, 2:3].astype(np.float32)
+        return radii, 2.0 * radii, counts
+
+
+class _StandInDistanceEngine:
+    def __init__(self, vertices, faces, **kw):
+        self.engine = _StandInEngine()
+
+
+def _mesh():
+    m = folded_icosphere(3, seed=2, jitter=0.1)
+    return m.vertices, m.faces, m.cortex_mask
+
+
+def _arrays(a):
+    out = {"msd_u": a.msd_unweighted, "msd_w": a.msd_weighted, "dist_b": a.dist_to_boundary,
+           "flag": a.field_flag, "indptr": a.sample_indptr, "radii": a.sample_radii_flat, "areas": a.sample_areas_flat}
+    for s in SCALES:
+        out[f"r{s}"] = a.radius_function[s]
+        out[f"p{s}"] = a.perimeter_function[s]
+    return out
+
+
+def _run(world_rank=None):
+    import warnings
+
+    from fastcorticalwiring_b200 import analysis, sharded
+
+    analysis.B200DistanceEngine = _StandInDistanceEngine
+    a = sharded.ShardedWiringAnalysis(*_mesh())
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)  # the stand-in flags some fields
+        a.compute_all_wiring_costs(scale=list(SCALES), n_samples_between_scales=2)
+    return _arrays(a), a.distance_engine.engine.seen
+
+
+def _rank(rank, world, port, q):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        arrays, seen = _run()
+        q.put((rank, arrays, seen))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_two_ranks_match_one_process():
+    from fastcorticalwiring_b200 import mesh as M, sharded
+
+    one, seen_one = _run()
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = sorted((q.get(timeout=180) for _ in range(world)), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    # every source computed once, each rank its contiguous slice of the BFS order
+    order = M.prepare(*_mesh()).bfs
+    assert np.array_equal(np.concatenate([np.asarray(s) for _, _, s in got]), order)
+    assert np.array_equal(np.asarray(seen_one), order)
+    for r, (_, _, seen) in enumerate(got):
+        assert np.array_equal(np.asarray(seen), sharded.shard(order, world, r))
+    for _, arrays, _ in got:
+        for k, v in one.items():
+            assert np.array_equal(arrays[k], v, equal_nan=True), k
+
+
+def test_shard_slices():
+    from fastcorticalwiring_b200 import sharded
+
+    order = np.arange(10)
+    parts = [sharded.shard(order, 3, r) for r in range(3)]
+    assert [p.tolist() for p in parts] == [[0, 1, 2, 3], [4, 5, 6], [7, 8, 9]]
+    assert np.array_equal(sharded.gather_rows(np.ones((2, 3))), np.ones((2, 3)))  # no process group
+    import pytest
+
+    with pytest.raises(ValueError):
+        sharded.shard(order, 2, 2)
