@@ -1423,14 +1423,9 @@ int narrow_ready(fcw_engine* e) {
     return FCW_OK;
 }
 
-}  // namespace
-
-int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host) {
-    FCW_TRY(check_engine(e));
-    if (!out_host) return fail(FCW_E_INVALID, "NULL argument");
-    if (source < 0 || source >= e->sym.n)
-        return fail(FCW_E_INVALID, "source_idx out of range: " + std::to_string(source) + " for mesh with " +
-                                       std::to_string(e->sym.n) + " vertices");
+// The drop-in chain for one source (in range) on e->stream: its path's task list to the
+// device, then the chain (the captured graph, or direct launches).
+int narrow_run(fcw_engine* e, int32_t source) {
     FCW_TRY(narrow_ready(e));
     NarrowState& q = e->nar;
     cudaStream_t st = e->stream;
@@ -1450,6 +1445,44 @@ int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host) {
     if (q.exec && e->graphs_on && !e->prof_on) FCW_CUDA(cudaGraphLaunch(q.exec, st));
     else FCW_TRY(narrow_chain(e, st));
     e->launches += q.launches;
+    return FCW_OK;
+}
+
+// fcw_compute_metrics for one source in FP64: the drop-in chain, then the statistics and
+// the per-source kernel at one column (records identical in meaning to the batched path's).
+int narrow_metrics(fcw_engine* e, int32_t source, const double* targets, int32_t nt, int32_t nb, double eps,
+                   double* out_host) {
+    e->sync_streams();  // the workspace's metric scratch may still be in use by a device-API call
+    const int32_t stride = fcw_metrics_stride(nt, nb);
+    FCW_TRY(ensure_workspace(e, fcw::kRhsTile, stride));
+    fcw::MetricArgs a;
+    FCW_TRY(metric_args(e, targets, nt, nb, eps, 1, a));
+    FCW_TRY(narrow_run(e, source));
+    NarrowState& q = e->nar;
+    cudaStream_t st = e->stream;
+    const int64_t n = e->sym.n, nu = std::max<int64_t>(e->n_urows, 1);
+    const double* X_p = q.pend + 2 * nu + n;  // the Poisson solution (elimination order)
+    a.src = q.order;                           // its first entry: the source's elimination index
+    fcw::launch_shift_stats_one(a, X_p, e->cw().dT64, st);
+    fcw::launch_source_metrics<double>(a, e->cw().dT64, st);
+    e->launches += 2;
+    FCW_CUDA(cudaGetLastError());
+    FCW_CUDA(cudaMemcpyAsync(out_host, a.out, (size_t)stride * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FCW_CUDA(cudaStreamSynchronize(st));
+    return check_kernel_errors(e, "metrics");
+}
+
+}  // namespace
+
+int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host) {
+    FCW_TRY(check_engine(e));
+    if (!out_host) return fail(FCW_E_INVALID, "NULL argument");
+    if (source < 0 || source >= e->sym.n)
+        return fail(FCW_E_INVALID, "source_idx out of range: " + std::to_string(source) + " for mesh with " +
+                                       std::to_string(e->sym.n) + " vertices");
+    FCW_TRY(narrow_run(e, source));
+    NarrowState& q = e->nar;
+    cudaStream_t st = e->stream;
     FCW_CUDA(cudaMemcpyAsync(out_host, q.out, (size_t)e->sym.n * sizeof(double), cudaMemcpyDeviceToHost, st));
     FCW_CUDA(cudaStreamSynchronize(st));
     return check_kernel_errors(e, "distance");
@@ -1533,6 +1566,7 @@ int fcw_compute_metrics(fcw_engine* e, const int32_t* sources, int64_t n, int32_
         if (sources[k] < 0 || sources[k] >= e->sym.n)
             return fail(FCW_E_INVALID, "source_idx out of range: " + std::to_string(sources[k]) + " for mesh with " +
                                            std::to_string(e->sym.n) + " vertices");
+    if (n == 1 && precision == FCW_PREC_FP64) return narrow_metrics(e, sources[0], targets, nt, nb, eps, out_host);
     const int32_t stride = fcw_metrics_stride(nt, nb);
     if (e->hcap_src < n) {
         if (e->hsrc_d) e->release(e->hsrc_d);

@@ -280,6 +280,8 @@ void launch_assemble_samples(const SampleArgs& a, cudaStream_t st);
 // partials and the per-source near-vertex lists.
 template <typename Tin, typename Tout>
 void launch_shift_stats(const MetricArgs& a, int32_t K, const Tin* phi, Tout* dT, cudaStream_t st);
+// The same for one field (K = 1): phi (n, elimination order) shifted at a.src[0] into d.
+void launch_shift_stats_one(const MetricArgs& a, const double* phi, double* d, cudaStream_t st);
 // Health, MSD, distance to boundary, radii, perimeters and samples of each source's field.
 template <typename T>
 void launch_source_metrics(const MetricArgs& a, const T* dT, cudaStream_t st);

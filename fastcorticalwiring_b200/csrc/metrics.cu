@@ -43,6 +43,44 @@ __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a,
 // Per-(vertex tile, source) partial statistics written by k_shift_stats.
 enum { P_SUM_D, P_SUM_DA, P_SUM_A, P_CNT, P_NEG, P_VIOL, P_NONFINITE, P_DMAX, P_N };
 
+// One vertex's share of the health screen and MSD sums (lean_geometry.py:343-357,
+// core_analysis.py:1573-1581) for the distance di at a vertex (vx, vy, vz) of area va from
+// a source at (sx, sy, sz): counts of non-finite values, of d < -h and of d < 0.9 |x - x_s| - h,
+// the valid-distance sums and the maximum. The chord test compares squares and takes the
+// reference's sqrt form only within a 1e-10 band of the threshold, so the counts match the
+// reference exactly. Returns whether the vertex is nearer than R0.
+__device__ __forceinline__ bool vertex_stats(double di, double vx, double vy, double vz, double va, double sx,
+                                             double sy, double sz, double h, double eps, double R0, double& sd,
+                                             double& sda, double& sa, double& dm, int& cnt, int& ng, int& vi,
+                                             int& nf) {
+    if (!isfinite(di)) {
+        ++nf;
+        return false;
+    }
+    if (di < -h) ++ng;
+    const double dx = vx - sx, dy = vy - sy, dz = vz - sz;
+    const double c2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+    const double t = di + h;
+    bool viol;
+    if (t < 0.0) {
+        viol = true;
+    } else {
+        const double lhs = t * t, rhs = 0.81 * c2;
+        if (lhs < rhs * (1.0 - 1e-10)) viol = true;
+        else if (lhs > rhs * (1.0 + 1e-10)) viol = false;
+        else viol = di < __dsub_rn(dmul(0.9, __dsqrt_rn(c2)), h);
+    }
+    if (viol) ++vi;
+    if (di > eps) {
+        sd += di;
+        sda += di * va;
+        sa += va;
+        ++cnt;
+    }
+    dm = fmax(dm, di);
+    return di < R0;
+}
+
 // The shift + transpose of one kStatVTile-vertex x 32-source tile, fused with the per-vertex
 // work of the health screen and MSD (lean_geometry.py:343-357, core_analysis.py:1573-1581):
 // counts of d < -h and of d < 0.9 |x - x_s| - h, the valid-distance sums and the maximum.
@@ -113,35 +151,8 @@ __global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K,
             if (in) dT[(int64_t)k * n + v] = dv;
             if (srcv[r] < 0) continue;  // warp-uniform (one source per warp)
             const double di = (double)dv;
-            bool near = false;
-            if (in) {
-                if (!isfinite(di)) {
-                    ++nf[j];
-                } else {
-                    if (di < -h) ++ng[j];
-                    const double dx = vx - sc[r][0], dy = vy - sc[r][1], dz = vz - sc[r][2];
-                    const double c2 = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-                    const double t = di + h;
-                    bool viol;
-                    if (t < 0.0) {
-                        viol = true;
-                    } else {
-                        const double lhs = t * t, rhs = 0.81 * c2;
-                        if (lhs < rhs * (1.0 - 1e-10)) viol = true;
-                        else if (lhs > rhs * (1.0 + 1e-10)) viol = false;
-                        else viol = di < __dsub_rn(dmul(0.9, __dsqrt_rn(c2)), h);
-                    }
-                    if (viol) ++vi[j];
-                    if (di > a.eps) {
-                        sd[j] += di;
-                        sda[j] += di * va;
-                        sa[j] += va;
-                        ++cnt[j];
-                    }
-                    dm[j] = fmax(dm[j], di);
-                    near = di < R0;
-                }
-            }
+            const bool near = in && vertex_stats(di, vx, vy, vz, va, sc[r][0], sc[r][1], sc[r][2], h, a.eps, R0,
+                                                 sd[j], sda[j], sa[j], dm[j], cnt[j], ng[j], vi[j], nf[j]);
             const unsigned mask = __ballot_sync(0xffffffffu, near);
             if (tx == 0) nearmask[r][sub] = mask;
         }
@@ -191,6 +202,87 @@ __global__ void __launch_bounds__(256, 3) k_shift_stats(MetricArgs a, int32_t K,
             if (m & (1u << tx))
                 a.near_list[(int64_t)k * n + base + off + __popc(m & lanes_below)] = vbase + sb * 32 + tx;
         }
+    }
+}
+
+// One field (the single-source path): the same shift, statistics and near list for the one
+// column of phi (n, elimination order) into d. A CTA takes kStatVTile vertices, a warp 32
+// consecutive ones per step; the tile's near vertices are appended in vertex order with one
+// atomic, as k_shift_stats appends them.
+__global__ void __launch_bounds__(256) k_shift_stats_one(MetricArgs a, const double* __restrict__ phi,
+                                                         double* __restrict__ d) {
+    constexpr int NG = kStatVTile / 32;  // 32-vertex groups of a tile
+    static_assert(NG == 32, "one lane per group in the near-list scan");
+    __shared__ unsigned gmask[NG];
+    __shared__ int gbase[NG];
+    __shared__ double wred[8][4];
+    __shared__ int wcnt[8][4];
+    __shared__ int base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = a.n, vbase = blockIdx.x * kStatVTile;
+    const int se = a.src[0];
+    const double p0 = phi[se];
+    const double sx = a.coords[3 * (int64_t)se], sy = a.coords[3 * (int64_t)se + 1], sz = a.coords[3 * (int64_t)se + 2];
+    double sd = 0.0, sda = 0.0, sa = 0.0, dm = 0.0;
+    int cnt = 0, ng = 0, vi = 0, nf = 0;
+    for (int g = warp; g < NG; g += 8) {
+        const int v = vbase + 32 * g + lane;
+        bool near = false;
+        if (v < n) {
+            const double dv = phi[v] - p0;
+            d[v] = dv;
+            near = vertex_stats(dv, a.coords[3 * (int64_t)v], a.coords[3 * (int64_t)v + 1],
+                                a.coords[3 * (int64_t)v + 2], a.vertex_area[v], sx, sy, sz, a.health_h, a.eps,
+                                a.near_radius, sd, sda, sa, dm, cnt, ng, vi, nf);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, near);
+        if (lane == 0) gmask[g] = m;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sd += __shfl_down_sync(0xffffffffu, sd, off);
+        sda += __shfl_down_sync(0xffffffffu, sda, off);
+        sa += __shfl_down_sync(0xffffffffu, sa, off);
+        dm = fmax(dm, __shfl_down_sync(0xffffffffu, dm, off));
+        cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+        ng += __shfl_down_sync(0xffffffffu, ng, off);
+        vi += __shfl_down_sync(0xffffffffu, vi, off);
+        nf += __shfl_down_sync(0xffffffffu, nf, off);
+    }
+    if (lane == 0) {
+        wred[warp][0] = sd; wred[warp][1] = sda; wred[warp][2] = sa; wred[warp][3] = dm;
+        wcnt[warp][0] = cnt; wcnt[warp][1] = ng; wcnt[warp][2] = vi; wcnt[warp][3] = nf;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // the tile's partials, the warps' sums added in warp order
+        if (lane == 0) {
+            double q[P_N] = {0.0};
+            for (int w = 0; w < 8; ++w) {
+                q[P_SUM_D] += wred[w][0]; q[P_SUM_DA] += wred[w][1]; q[P_SUM_A] += wred[w][2];
+                q[P_DMAX] = fmax(q[P_DMAX], wred[w][3]);
+                q[P_CNT] += wcnt[w][0]; q[P_NEG] += wcnt[w][1]; q[P_VIOL] += wcnt[w][2]; q[P_NONFINITE] += wcnt[w][3];
+            }
+            double* o = a.partials + (int64_t)blockIdx.x * P_N;
+            for (int i = 0; i < P_N; ++i) o[i] = q[i];
+        }
+        // group offsets of the near list, in vertex order (NG = 32 groups: one per lane)
+        const int c = __popc(gmask[lane]);
+        int incl = c;
+        for (int off = 1; off < 32; off <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += t;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        int b = 0;
+        if (lane == 0 && total > 0) b = atomicAdd(a.near_count, total);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        gbase[lane] = b + incl - c;
+    }
+    __syncthreads();
+    const unsigned below = (1u << lane) - 1u;
+    for (int g = warp; g < NG; g += 8) {
+        const unsigned m = gmask[g];
+        if (m & (1u << lane)) a.near_list[gbase[g] + __popc(m & below)] = vbase + 32 * g + lane;
     }
 }
 
@@ -777,6 +869,12 @@ void launch_shift_stats(const MetricArgs& a, int32_t K, const Tin* phi, Tout* dT
     if (a.n <= 0 || K <= 0) return;
     cudaMemsetAsync(a.near_count, 0, (size_t)K * sizeof(int), st);
     k_shift_stats<Tin, Tout><<<dim3(a.ntiles, K / 32), dim3(32, 8), 0, st>>>(a, K, phi, dT);
+}
+
+void launch_shift_stats_one(const MetricArgs& a, const double* phi, double* d, cudaStream_t st) {
+    if (a.n <= 0) return;
+    cudaMemsetAsync(a.near_count, 0, sizeof(int), st);
+    k_shift_stats_one<<<a.ntiles, 256, 0, st>>>(a, phi, d);
 }
 
 template <typename T>

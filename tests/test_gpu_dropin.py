@@ -77,3 +77,24 @@ def test_dropin_rejects_bad_source_and_recovers(l6):
             eng.compute_distance(bad)
     d = eng.compute_distance(picks[0])
     assert d[picks[0]] == 0.0 and np.all(np.isfinite(d))
+
+
+def test_single_source_metrics_match_batched(l6):
+    """compute_metrics on one source in FP64 runs the drop-in chain and one-column statistics;
+    its records must equal the batched path's for the same sources (two schedules of the same
+    FP64 solve: to 1e-10 relative; flags and counts exactly)."""
+    pm, eng, picks = l6
+    targets = pm.targets(M.RUNNER_SCALES)
+    sel = np.asarray(picks[:6], np.int32)
+    batched = engine.split_records(eng.compute_metrics(sel, targets, precision="fp64"), targets.size, 3)
+    for j, s in enumerate(sel):
+        one = engine.split_records(eng.compute_metrics(np.array([s], np.int32), targets, precision="fp64"),
+                                   targets.size, 3)
+        assert bool(one["bad"][0]) == bool(batched["bad"][j])
+        if batched["bad"][j]:
+            continue
+        for key in ("radii", "perim", "msd_u", "msd_w", "dist_b", "extra_r", "extra_a"):
+            a, b = np.asarray(one[key][0], float), np.asarray(batched[key][j], float)
+            ok = np.isfinite(b)
+            assert np.array_equal(np.isfinite(a), ok), key
+            assert np.all(np.abs(a[ok] - b[ok]) <= 1e-10 * np.abs(b[ok])), key
