@@ -98,3 +98,21 @@ def test_single_source_metrics_match_batched(l6):
             ok = np.isfinite(b)
             assert np.array_equal(np.isfinite(a), ok), key
             assert np.all(np.abs(a[ok] - b[ok]) <= 1e-10 * np.abs(b[ok])), key
+
+
+@pytest.mark.parametrize("level,jitter,robust", [(5, 0.2, True), (8, 0.2, False)])
+def test_dropin_matches_batched_on_other_meshes(level, jitter, robust):
+    """The drop-in chain on the robust (intrinsic Delaunay) operators and on the L8 mesh (59
+    etree levels, the deepest measured), against the batched FP64 path of the same engine."""
+    m = folded_icosphere(level, seed=1, jitter=jitter)
+    pm = M.prepare(m.vertices, m.faces, m.cortex_mask)
+    eng = engine.HeatEngine(pm.V, pm.F, robust=int(robust), block_k=64)
+    try:
+        picks = [int(x) for x in pm.bfs[np.linspace(0, pm.n_vertices - 1, 3).astype(int)]]
+        batched = eng.compute_distances(np.asarray(picks, np.int32), precision="fp64")
+        for j, s in enumerate(picks):
+            d = eng.compute_distance(s)
+            assert d[s] == 0.0
+            assert _maxrel(d, batched[j]) <= 1e-12, (level, s, _maxrel(d, batched[j]))
+    finally:
+        eng.close()
