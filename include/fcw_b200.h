@@ -147,7 +147,11 @@ int fcw_engine_destroy(fcw_engine* e);
 
 /* One source, FP64 heat method, result in host memory (n_vertices doubles),
  * shifted so that d[source] = 0. Replaces BaseDistanceEngine.compute_distance
- * (distance_engines.py:67-69, 131-133). */
+ * (distance_engines.py:67-69, 131-133). Runs its own chain (one-column sweeps);
+ * the first call on an engine builds that chain's panel layouts (four arrays of
+ * one factor's size) and captures it as a CUDA graph, so it should come before
+ * any capture of the engine's stream. Copies run at full speed into page-locked
+ * out_host. A source out of range is FCW_E_INVALID. */
 int fcw_compute_distance(fcw_engine* e, int32_t source, double* out_host);
 
 /* Distances for n sources into host memory, row j = distances from sources[j]
