@@ -61,7 +61,7 @@ def _arrays(a):
     return out
 
 
-def _run(world_rank=None):
+def _run(subset=None):
     import warnings
 
     from fastcorticalwiring_b200 import analysis, sharded
@@ -70,8 +70,14 @@ def _run(world_rank=None):
     a = sharded.ShardedWiringAnalysis(*_mesh())
     with warnings.catch_warnings():
         warnings.simplefilter("ignore", RuntimeWarning)  # the stand-in flags some fields
-        a.compute_all_wiring_costs(scale=list(SCALES), n_samples_between_scales=2)
+        a.compute_all_wiring_costs(scale=list(SCALES), n_samples_between_scales=2, vertex_subset=subset)
     return _arrays(a), a.distance_engine.engine.seen
+
+
+def _subset():
+    """Every third original vertex (the reference's vertex_subset, core_analysis.py:1519-1533)."""
+    m = _mesh()
+    return list(range(0, m[0].shape[0], 3))
 
 
 def _rank(rank, world, port, q):
@@ -82,7 +88,8 @@ def _rank(rank, world, port, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         arrays, seen = _run()
-        q.put((rank, arrays, seen))
+        sub_arrays, sub_seen = _run(_subset())
+        q.put((rank, arrays, seen, sub_arrays, sub_seen))
     finally:
         dist.destroy_process_group()
 
@@ -97,6 +104,7 @@ def test_two_ranks_match_one_process():
     from fastcorticalwiring_b200 import mesh as M, sharded
 
     one, seen_one = _run()
+    sub_one, _ = _run(_subset())
     world = 2
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -110,13 +118,16 @@ def test_two_ranks_match_one_process():
         assert p.exitcode == 0
     # every source computed once, each rank its contiguous slice of the BFS order
     order = M.prepare(*_mesh()).bfs
-    assert np.array_equal(np.concatenate([np.asarray(s) for _, _, s in got]), order)
+    assert np.array_equal(np.concatenate([np.asarray(g[2]) for g in got]), order)
     assert np.array_equal(np.asarray(seen_one), order)
-    for r, (_, _, seen) in enumerate(got):
-        assert np.array_equal(np.asarray(seen), sharded.shard(order, world, r))
-    for _, arrays, _ in got:
+    for r, g in enumerate(got):
+        assert np.array_equal(np.asarray(g[2]), sharded.shard(order, world, r))
+    for g in got:
         for k, v in one.items():
-            assert np.array_equal(arrays[k], v, equal_nan=True), k
+            assert np.array_equal(g[1][k], v, equal_nan=True), k
+        for k, v in sub_one.items():  # a vertex subset shards the same way
+            assert np.array_equal(g[3][k], v, equal_nan=True), k
+    assert sum(len(g[4]) for g in got) < order.size  # only the subset's sources were computed
 
 
 def test_shard_slices():
