@@ -349,8 +349,8 @@ struct SrcShared {
         double pre[kMaxBins + 1];               // then the exclusive prefix sums of the sub-bins' areas
     };
     int ptr[kMaxBins + 1];     // faces per sub-bin -> exclusive prefix -> (counting sort) inclusive prefix
-    double red[16][4];
-    double dred[16][5];
+    double red[32][4];         // per warp (up to 1024 threads)
+    double dred[32][5];
     double radii[kMaxTargets];
     double total, dglob;
     int minlo[kMaxBins + 1];   // per sub-bin: a lower bound of its faces' lo (lo_key), then the suffix minima
@@ -554,8 +554,8 @@ struct Field {
 //      two bins below rc, rc grows (to the near lists' radius, then up to every bin,
 //      scanning all vertices) and step 2 repeats;
 //   3. one warp per target: bracket + safeguarded Newton + perimeter; then the samples.
-template <typename T>
-__global__ void __launch_bounds__(kMetricThreads, 4) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_source_metrics(MetricArgs a, const T* __restrict__ dT) {
     __shared__ SrcShared S;
     const int k = blockIdx.x;
     const int src = a.src[k];
@@ -880,7 +880,10 @@ void launch_shift_stats_one(const MetricArgs& a, const double* phi, double* d, c
 template <typename T>
 void launch_source_metrics(const MetricArgs& a, const T* dT, cudaStream_t st) {
     if (a.nsrc <= 0) return;
-    k_source_metrics<T><<<a.nsrc, kMetricThreads, 0, st>>>(a, dT);
+    // a lone source (the single-source path) gets a CTA of 1024 threads: its binning, sort and
+    // targets spread over 32 warps instead of waiting on one CTA's 8
+    if (a.nsrc == 1) k_source_metrics<T, 1024><<<1, 1024, 0, st>>>(a, dT);
+    else k_source_metrics<T, kMetricThreads><<<a.nsrc, kMetricThreads, 0, st>>>(a, dT);
 }
 
 template void launch_shift_transpose<double, double>(int32_t, int32_t, const double*, const int32_t*, double*,
