@@ -762,7 +762,7 @@ int ensure_one(fcw_engine* e, Workspace& w, int32_t K, int32_t stride) {
     FCW_TRY(e->dalloc(&w.dT64, (size_t)n * Kn));
     w.dT32 = reinterpret_cast<float*>(w.dT64);
     FCW_TRY(e->dalloc(&w.src, (size_t)Kn));
-    FCW_TRY(e->dalloc(&w.reach, (size_t)std::max<int64_t>(e->sym.nsuper, 1)));
+    FCW_TRY(e->dalloc(&w.reach, (size_t)std::max<int64_t>(e->sym.nsuper, 1) * (Kn / fcw::kReachCols)));
     FCW_TRY(e->dalloc(&w.band, (size_t)nf * Kn));
     FCW_TRY(e->dalloc(&w.longf, (size_t)nf * Kn));
     FCW_TRY(e->dalloc(&w.out, (size_t)sn * Kn));
@@ -861,6 +861,7 @@ void heat_solve(fcw_engine* e, int32_t K, cudaStream_t st) {
     fcw::SolveArgs<double> a = solve_args<double>(e, e->val_h, e->inv_h, w.Bh, K);
     a.delta_src = w.src;
     a.reach = w.reach;
+    a.reach_tiles = K / fcw::kReachCols;
     sweep<double>(e, a, st, FCW_STAGE_HEAT_FWD, FCW_STAGE_HEAT_BWD);
 }
 

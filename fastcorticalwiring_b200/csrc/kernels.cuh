@@ -61,6 +61,7 @@ void launch_panel_inverse(const DevPlan& p, double* val, const double* inv, cuda
 
 // ---- multi-RHS supernodal triangular solves (solve.cu) ----
 constexpr int kRhsTile = 64;     // right-hand sides per solve CTA; K is a multiple of this
+constexpr int kReachCols = 64;   // columns per tile of the heat solve's reach flags (its FP64 tile width)
 constexpr int kSplitRows = 128;  // structure rows per backward split-K task
 
 template <typename T>
@@ -77,7 +78,9 @@ struct SolveArgs {
     const int32_t* gm_src = nullptr;
     const int32_t* gm_child = nullptr;
     const int32_t* delta_src = nullptr;  // forward: identity columns for these sources (elimination order)
-    const uint8_t* reach = nullptr;      // supernodes on a source's path to the root (heat solve)
+    const uint8_t* reach = nullptr;      // heat solve: reach[s * reach_tiles + t], supernode s on the path to the
+                                         // root of some source of column tile t (kReachCols columns)
+    int32_t reach_tiles = 0;
     const int2* tasks = nullptr;         // (supernode, row chunk | split)
     const int32_t* nsplit = nullptr;     // backward splits per supernode
     const int64_t* poff = nullptr;       // partial-sum slot of the first split (units of 64 x K)

@@ -39,7 +39,8 @@
 //
 // Heat right-hand sides are columns of the identity: the forward sweep builds
 // them from the source list, and only supernodes on a source's path to the
-// root (`reach`) are solved; the others' forward results are zero.
+// root (`reach`, per supernode and 64-column tile) are solved; the others' forward results
+// are zero.
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -394,9 +395,10 @@ __global__ void __launch_bounds__(NT, 3) k_fwd(SolveArgs<T> a, int32_t t0) {
     T* St = Pn + TR * LA;                   // a.stage x KT: children's update rows
     __shared__ int grs[TR + 1];
     __shared__ unsigned char live[stage_rows<T, TR>()];
+    static_assert(sizeof(T) == 4 || KT == kReachCols, "the heat solve's reach tiles are its column tiles");
     const int2 task = a.tasks[t0 + blockIdx.x];
     const int s = task.x, chunk = task.y;
-    if (a.reach && !a.reach[s]) return;
+    if (a.reach && !a.reach[(int64_t)s * a.reach_tiles + blockIdx.y]) return;
     const DevPlan& p = a.p;
     const int tid = threadIdx.x;
     const int K = a.K, k0 = blockIdx.y * KT;
@@ -485,6 +487,7 @@ __global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
     constexpr int VPR = KT / vec<T>(), LW = ld_rows<T, KT>(), LA = ld_bwd_a<T, TR>(), DP = depth_pad<T>();
     constexpr int PS = RC * LA, XS = RC * LW;  // one chunk buffer: panel rows, gathered solution rows
     static_assert(2 * (PS + XS) >= TR * LW + TR * LA, "the finishing tiles alias the chunk buffers");
+    static_assert(sizeof(T) == 4 || KT == kReachCols, "the heat solve's reach tiles are its column tiles");
     using AccT = Acc<T, KT, TR>;
     extern __shared__ __align__(16) unsigned char smraw[];
     T* buf = reinterpret_cast<T*>(smraw);
@@ -540,7 +543,7 @@ __global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
         __syncthreads();
     }
 
-    const bool zero_y = a.reach && !a.reach[s];
+    const bool zero_y = a.reach && !a.reach[(int64_t)s * a.reach_tiles + blockIdx.y];
     if (nspl > 1) {
         T* part = a.part + a.poff[s] * (int64_t)PT * K + k0;
         T* mine = part + (int64_t)split * PT * K;
@@ -609,16 +612,20 @@ __global__ void __launch_bounds__(NT, 3) k_bwd(SolveArgs<T> a, int32_t t0) {
     acc.visit(ns, [&](int r, int c, T* v) { st_n<T, AccT::V>(out + (int64_t)r * K + c, v); });
 }
 
+// reach[s * tiles + t]: some source of column tile t (kReachCols columns) has supernode s on
+// its path to the root.
 __global__ void k_reach(const int32_t* __restrict__ col_sn, const int32_t* __restrict__ parent,
-                        const int32_t* __restrict__ src, int32_t K, int32_t nlevels, uint8_t* __restrict__ reach) {
+                        const int32_t* __restrict__ src, int32_t K, int32_t nlevels, int32_t tiles,
+                        uint8_t* __restrict__ reach) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K) return;
     const int s0 = src[k];
     if (s0 < 0) return;
+    const int t = k / kReachCols;
     int s = col_sn[s0];
     // the parent chain is strictly increasing and at most nlevels long
     for (int it = 0; s >= 0 && it <= nlevels; ++it) {
-        reach[s] = 1;
+        reach[(int64_t)s * tiles + t] = 1;
         s = parent[s];
     }
 }
@@ -688,8 +695,9 @@ void launch_bwd_level(const SolveArgs<T>& a, int32_t t0, int32_t ntasks, int32_t
 }
 
 void launch_reach(const DevPlan& p, const int32_t* src, int32_t K, uint8_t* reach, cudaStream_t st) {
-    cudaMemsetAsync(reach, 0, (size_t)p.nsuper, st);
-    k_reach<<<(K + 127) / 128, 128, 0, st>>>(p.col_sn, p.sn_parent, src, K, p.nlevels, reach);
+    const int32_t tiles = K / kReachCols;
+    cudaMemsetAsync(reach, 0, (size_t)p.nsuper * tiles, st);
+    k_reach<<<(K + 127) / 128, 128, 0, st>>>(p.col_sn, p.sn_parent, src, K, p.nlevels, tiles, reach);
 }
 
 template void launch_fwd_level<double>(const SolveArgs<double>&, int32_t, int32_t, bool, cudaStream_t);

@@ -111,7 +111,7 @@ __device__ __forceinline__ void gather_issue(const SolveArgs<T>& a, const Gather
     for (int i = threadIdx.x; i < ne * VPR; i += NT) {
         const int e = i / VPR, v = i - e * VPR;
         const int ge = g.eb + e0 + e;
-        const bool on = !a.reach || a.reach[a.gm_child[ge]];
+        const bool on = !a.reach || a.reach[(int64_t)a.gm_child[ge] * a.reach_tiles + k0 / kReachCols];
         if (v == 0) live[e] = on;
         if (on) copy16_async(St + e * KT + v * vec<T>(), a.U + (int64_t)a.gm_src[ge] * a.K + k0 + v * vec<T>());
     }
