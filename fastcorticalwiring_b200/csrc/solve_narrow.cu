@@ -125,10 +125,11 @@ __device__ __forceinline__ void wait_predecessor() { asm volatile("griddepcontro
 __host__ __device__ __forceinline__ int chunk_rows(int m, int c) { return min(CR, m - CR * c); }
 __host__ __device__ __forceinline__ int even(int x) { return (x + 1) & ~1; }
 
-// Task shapes of the host's task lists. A front of at most FC chunks is one forward task; a larger one (the separators near the root, on the
-// critical path) is one task per chunk, so its rows are formed in parallel. Backward
-// strips hold as many whole columns as fit, at most 8 (one per warp) for fronts of
-// more than 256 rows, in equal widths.
+// Task shapes of the host's task lists. A front of at most FC chunks is one forward
+// task; a larger one (the separators near the root, on the critical path) is one task
+// per chunk, so its rows are formed in parallel. Backward strips hold as many whole
+// columns as fit, at most 8 (one per warp) for fronts of more than 256 rows, in equal
+// widths.
 inline int fwd_chunks_per_task(int m) {
     const int nch = (m + CR - 1) / CR;
     return nch <= FC ? nch : 1;
