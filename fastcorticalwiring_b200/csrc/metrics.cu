@@ -217,7 +217,6 @@ __global__ void __launch_bounds__(256) k_shift_stats_one(MetricArgs a, const dou
     __shared__ int gbase[NG];
     __shared__ double wred[8][4];
     __shared__ int wcnt[8][4];
-    __shared__ int base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = a.n, vbase = blockIdx.x * kStatVTile;
     const int se = a.src[0];
