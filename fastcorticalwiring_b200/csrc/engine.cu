@@ -4,7 +4,8 @@
 // the host, runs the symbolic analysis, uploads the structure and factors the
 // heat operator M + tL and the Poisson operator L + shift*M in FP64 on the
 // device (plus, for the mixed form, the Poisson operator grounded at the last
-// eliminated vertex, rounded to FP32). A block of K sources then runs:
+// eliminated vertex of each connected component, rounded to FP32). A block of K
+// sources then runs:
 //   reach -> heat forward (delta RHS, pruned) -> heat backward -> divergence
 //   -> Poisson forward/backward -> shift + transpose -> vertex stats -> geometry
 // entirely on one stream.
@@ -122,6 +123,7 @@ struct Workspace {
     int32_t out_stride = 0;
     double* U = nullptr;        // forward update rows, (sum nr) x K doubles (reused as floats)
     double* partials = nullptr; // per (vertex tile, source) health/MSD partial sums
+    double* csum = nullptr;     // per (vertex tile, source) component sums, then the levels (several components)
     int32_t* near_list = nullptr;
     int32_t* near_count = nullptr;
     cudaStream_t stream = nullptr;  // this workspace's stream in the pipelined device path
@@ -174,7 +176,17 @@ struct fcw_engine {
     fcw::MeshPrep mesh;
     fcw::Symbolic sym;
     double t_coef = 0.0, t = 0.0;
-    int32_t ground_new = -1;
+    // the grounded (mixed-form) Poisson operator: one ground vertex per connected component of
+    // the submesh, its last eliminated vertex; flags in the caller's order (host) and in
+    // elimination order (device)
+    std::vector<uint8_t> grounded_old;
+    uint8_t* grounded_d = nullptr;
+    // with several components: each vertex's component and lumped mass (elimination order) and
+    // each component's total mass, for the mixed form's level on the source's component
+    int32_t ncomp = 1;
+    std::vector<int32_t> comp_h;
+    std::vector<double> cmass_h, carea_h;
+    fcw::ComponentLevel clevel;
     cudaStream_t stream = nullptr;
     std::vector<std::pair<void*, size_t>> allocs;  // device allocations and their sizes
     int64_t bytes = 0;
@@ -368,7 +380,6 @@ std::vector<double> operator_values(const fcw_engine* e, Op op) {
     const auto& S = e->sym;
     const auto& m = e->mesh;
     std::vector<double> v(S.nnz_lower_a);
-    const int32_t gold = e->ground_new >= 0 ? S.perm[e->ground_new] : -1;
     for (int64_t q = 0; q < S.nnz_lower_a; ++q) {
         const int64_t k = S.a_src[q];
         const int32_t col = S.a_col[q], row = m.Li[k];
@@ -381,8 +392,8 @@ std::vector<double> operator_values(const fcw_engine* e, Op op) {
             case Op::Poisson:  // L + shift M (fastcw_lean.py:500)
                 v[q] = diag ? L + e->prm.poisson_shift * m.mass[col] : L;
                 break;
-            case Op::Grounded:  // L with the ground vertex's row and column replaced by the identity
-                v[q] = (row == gold || col == gold) ? (diag ? 1.0 : 0.0) : L;
+            case Op::Grounded:  // L with the ground vertices' rows and columns replaced by the identity
+                v[q] = (e->grounded_old[row] || e->grounded_old[col]) ? (diag ? 1.0 : 0.0) : L;
                 break;
         }
     }
@@ -409,7 +420,47 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     const auto& S = e->sym;
     const auto& m = e->mesh;
     if (S.max_ns > fcw::kMaxWidth) return fail(FCW_E_INVALID, "supernode wider than the kernels support");
-    e->ground_new = (int32_t)(S.n - 1);
+    {
+        // connected components of the submesh (union-find over its faces), each grounded at its
+        // last eliminated vertex: L is singular once per component
+        std::vector<int32_t> up(S.n);
+        for (int64_t i = 0; i < S.n; ++i) up[i] = (int32_t)i;
+        auto find = [&](int32_t x) {
+            while (up[x] != x) x = up[x] = up[up[x]];
+            return x;
+        };
+        for (int64_t f = 0; f < m.nf; ++f)
+            for (int c = 1; c < 3; ++c) {
+                const int32_t a = find(m.F[3 * f]), b = find(m.F[3 * f + c]);
+                if (a != b) up[std::max(a, b)] = std::min(a, b);
+            }
+        std::vector<int32_t> last(S.n, -1);
+        for (int64_t i = 0; i < S.n; ++i) last[find(S.perm[i])] = (int32_t)i;  // ascending i: the last wins
+        e->grounded_old.assign(S.n, 0);
+        e->ncomp = 0;
+        for (int64_t v = 0; v < S.n; ++v)
+            if (last[v] >= 0) {
+                e->grounded_old[S.perm[last[v]]] = 1;
+                ++e->ncomp;
+            }
+        if (e->ncomp > 1) {
+            std::vector<int32_t> label(S.n, -1), comp(S.n);
+            std::vector<double> cmass(S.n), carea;
+            for (int64_t i = 0; i < S.n; ++i) {
+                const int32_t r = find(S.perm[i]);
+                if (label[r] < 0) {
+                    label[r] = (int32_t)carea.size();
+                    carea.push_back(0.0);
+                }
+                comp[i] = label[r];
+                cmass[i] = m.mass[S.perm[i]];
+                carea[label[r]] += cmass[i];
+            }
+            e->comp_h = std::move(comp);
+            e->cmass_h = std::move(cmass);
+            e->carea_h = std::move(carea);
+        }
+    }
 
     FCW_CUDA(cudaSetDevice(e->device));
     FCW_CUDA(cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, e->device));
@@ -645,6 +696,17 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     FCW_TRY(e->upload(&e->g12_d, m.g12));
     FCW_TRY(e->upload(&e->g22_d, m.g22));
     FCW_TRY(e->upload(&e->iperm_d, S.iperm));
+    {
+        std::vector<uint8_t> gnew(S.n);
+        for (int64_t i = 0; i < S.n; ++i) gnew[i] = e->grounded_old[S.perm[i]];
+        FCW_TRY(e->upload(&e->grounded_d, gnew));
+    }
+    if (e->ncomp > 1) {
+        e->clevel.n = (int32_t)S.n;
+        FCW_TRY(e->upload(&e->clevel.comp, e->comp_h));
+        FCW_TRY(e->upload(&e->clevel.mass, e->cmass_h));
+        FCW_TRY(e->upload(&e->clevel.area, e->carea_h));
+    }
     FCW_TRY(e->upload(&e->perm_d, S.perm));
 
     // numeric factorisations
@@ -675,7 +737,6 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     FCW_TRY(run_factor(Op::Poisson, e->val_p, e->inv_p, "Poisson factorisation"));
     if (e->prm.build_mixed && e->prm.refine > 0) {
         // L_g in CSR, elimination order: the entries the FP32 factor came from
-        const int32_t gold = S.perm[e->ground_new];
         std::vector<int64_t> rp(S.n + 1, 0);
         std::vector<int32_t> ci;
         std::vector<double> av;
@@ -686,7 +747,7 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
             for (int64_t k = m.Lp[old]; k < m.Lp[old + 1]; ++k) {
                 const int32_t j = m.Li[k];
                 const bool diag = j == old;
-                const double v = (old == gold || j == gold) ? (diag ? 1.0 : 0.0) : m.Lx[k];
+                const double v = (e->grounded_old[old] || e->grounded_old[j]) ? (diag ? 1.0 : 0.0) : m.Lx[k];
                 if (v == 0.0 && !diag) continue;
                 ci.push_back(S.iperm[j]);
                 av.push_back(v);
@@ -745,7 +806,7 @@ int ensure_one(fcw_engine* e, Workspace& w, int32_t K, int32_t stride) {
     const int32_t Kn = std::max(K, w.K);
     const int32_t sn = std::max(stride, w.out_stride);
     void* old[] = {w.Bh, w.Bp64, w.Y, w.dT64, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
-                   w.counters, w.partials, w.near_list, w.near_count, w.desc};
+                   w.counters, w.partials, w.near_list, w.near_count, w.desc, w.csum};
     for (void* p : old)
         if (p) e->release(p);
     w.drop_graph();  // its launches name the old buffers
@@ -776,6 +837,7 @@ int ensure_one(fcw_engine* e, Workspace& w, int32_t K, int32_t stride) {
     FCW_TRY(e->dalloc(&w.counters, (size_t)nctr));
     FCW_CUDA(cudaMemset(w.counters, 0, nctr * sizeof(int)));
     FCW_TRY(e->dalloc(&w.desc, 1));
+    if (e->ncomp > 1) FCW_TRY(e->dalloc(&w.csum, (size_t)(fcw::component_tiles(n) + 1) * Kn));
     w.K = Kn;
     w.out_stride = sn;
     return FCW_OK;
@@ -793,7 +855,7 @@ int ensure_workspace(fcw_engine* e, int32_t K, int32_t stride) {
         for (size_t j = i; j < e->pool.size(); ++j) {
             Workspace& w = e->pool[j];
             void* bufs[] = {w.Bh, w.Bp64, w.Y, w.dT64, w.src, w.reach, w.band, w.longf, w.out, w.U, w.part,
-                            w.counters, w.partials, w.near_list, w.near_count, w.desc};
+                            w.counters, w.partials, w.near_list, w.near_count, w.desc, w.csum};
             for (void* p : bufs)
                 if (p) e->release(p);
             w.drop_graph();
@@ -904,7 +966,7 @@ int distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, co
     mark(e, st, FCW_STAGE_DIVERGENCE);
     if (precision == FCW_PREC_MIXED) {
         float* Y = reinterpret_cast<float*>(w.Y);
-        fcw::launch_divergence_mixed(e->fd, w.Bh, w.Bp32, K, e->ground_new, st);
+        fcw::launch_divergence_mixed(e->fd, w.Bh, w.Bp32, K, e->grounded_d, st);
         FCW_TRY(poisson_solve<float>(e, e->val_g, e->inv_g, w.Bp32, Y, K, st));
         // refinement: residual in FP64 and its FP32 solution, in the shift's output buffer
         // (two n x K float halves of dT64) before the shift writes it
@@ -915,6 +977,10 @@ int distances_block(fcw_engine* e, int32_t K, int precision, cudaStream_t st, co
             FCW_TRY(poisson_solve<float>(e, e->val_g, e->inv_g, r, d, K, st));
             fcw::launch_add((int64_t)n * K, Y, d, e->num_sms, st);
             e->launches += 2;
+        }
+        if (e->ncomp > 1) {
+            fcw::launch_component_level(e->clevel, K, w.src, Y, w.csum, st);
+            e->launches += 3;
         }
         mark(e, st, FCW_STAGE_SHIFT);
         if (ma) fcw::launch_shift_stats<float, float>(*ma, K, Y, w.dT32, st);

@@ -89,7 +89,8 @@ __device__ __forceinline__ double unit_scale(double m) {
 // once, lane j holding the j-th, and broadcast face by face.
 template <int NP>
 __global__ void __launch_bounds__(256) k_div_mixed(FaceData fd, const double* __restrict__ u,
-                                                   float* __restrict__ div, int32_t K, int32_t ground) {
+                                                   float* __restrict__ div, int32_t K,
+                                                   const uint8_t* __restrict__ grounded) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int v = blockIdx.x * 8 + warp;
     if (v >= fd.nv) return;
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(256) k_div_mixed(FaceData fd, const double* __
     float acc[2 * NP];
 #pragma unroll
     for (int t = 0; t < 2 * NP; ++t) acc[t] = 0.0f;
-    if (v != ground) {
+    if (!grounded[v]) {
         const int q0 = fd.inc_ptr[v], deg = fd.inc_ptr[v + 1] - q0;
         for (int jb = 0; jb < deg; jb += 32) {
             const int nj = min(32, deg - jb);
@@ -163,13 +164,13 @@ void launch_divergence_fp64_one(const FaceData& fd, const double* u, double* div
     if (fd.nv > 0) k_div_fp64_one<<<(fd.nv + 255) / 256, 256, 0, st>>>(fd, u, div);
 }
 
-void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,
+void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, const uint8_t* grounded,
                              cudaStream_t st) {
     if (fd.nv <= 0 || K <= 0) return;
     if (K % 128 == 0)
-        k_div_mixed<2><<<dim3((fd.nv + 7) / 8, K / 128), 256, 0, st>>>(fd, u, div, K, ground);
+        k_div_mixed<2><<<dim3((fd.nv + 7) / 8, K / 128), 256, 0, st>>>(fd, u, div, K, grounded);
     else  // K is a multiple of 64
-        k_div_mixed<1><<<dim3((fd.nv + 7) / 8, K / 64), 256, 0, st>>>(fd, u, div, K, ground);
+        k_div_mixed<1><<<dim3((fd.nv + 7) / 8, K / 64), 256, 0, st>>>(fd, u, div, K, grounded);
 }
 
 }  // namespace fcw

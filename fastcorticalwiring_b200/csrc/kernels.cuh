@@ -189,6 +189,21 @@ void launch_residual(const CsrOperator& A, int32_t K, const float* b, const floa
 // y += d over count floats (a multiple of 4)
 void launch_add(int64_t count, float* y, const float* d, int num_sms, cudaStream_t st);
 
+// ---- the mixed form's level on a submesh of several connected components (refine.cu) ----
+struct ComponentLevel {
+    int32_t n = 0;
+    int32_t* comp = nullptr;  // n: each vertex's component (elimination order)
+    double* mass = nullptr;   // n: each vertex's lumped mass (elimination order)
+    double* area = nullptr;   // each component's total lumped mass
+};
+// vertex tiles of the level's per-tile sums
+int64_t component_tiles(int64_t n);
+// Sets each column of phi (n x K FP32, row-major, zero off its source's component) off the
+// component of its source src[k] (elimination order) to the M-weighted mean of phi over that
+// component. scratch: (component_tiles(n) + 1) * K doubles. Three kernels.
+void launch_component_level(const ComponentLevel& c, int32_t K, const int32_t* src, float* phi, double* scratch,
+                            cudaStream_t st);
+
 // ---- fused gradient -> normalise -> divergence (face.cu) ----
 struct FaceData {
     int32_t nv = 0, nf = 0;
@@ -209,7 +224,8 @@ struct FaceData {
 void launch_divergence_fp64(const FaceData& fd, const double* u, double* div, int32_t K, cudaStream_t st);
 // One column (K = 1), the same arithmetic per vertex.
 void launch_divergence_fp64_one(const FaceData& fd, const double* u, double* div, cudaStream_t st);
-void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, int32_t ground,
+// grounded (elimination order): the ground vertices, whose divergence is zero
+void launch_divergence_mixed(const FaceData& fd, const double* u, float* div, int32_t K, const uint8_t* grounded,
                              cudaStream_t st);
 
 // ---- per-source kernels (metrics.cu) ----

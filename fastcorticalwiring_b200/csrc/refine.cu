@@ -6,6 +6,14 @@
 // the FP64 operator the factor came from, so r is the true residual rounded once to
 // FP32), solves L_g d = r with the same FP32 factor and adds d: the error shrinks by about
 // the factor's relative error, to the FP32 storage of phi.
+//
+// On a submesh of several connected components, L is singular once per component and the
+// grounded operator fixes one vertex of each at zero. The FP64 form's L + shift*M instead
+// leaves phi with zero M-weighted mean on the source's component (1^T div X = 0 there) and
+// zero on the others (no heat reaches them), so after the shift phi - phi(s) the vertices of
+// other components sit at the mean distance over the source's component. The component level
+// gives the grounded solution the same values off the source's component; on it the shift
+// removes the difference.
 #include "kernels.cuh"
 
 namespace fcw {
@@ -44,7 +52,84 @@ __global__ void k_add(int64_t n4, float4* __restrict__ y, const float4* __restri
     }
 }
 
+constexpr int kCompVTile = 256;
+
+// part[tile][k] = sum over the tile's vertices v in the component of src[k] of mass[v] phi[v][k].
+// 32 sources x 8 vertex rows per CTA: each warp reads 128 contiguous bytes of a row.
+__global__ void __launch_bounds__(256) k_comp_partial(int32_t n, int32_t K, const int32_t* __restrict__ src,
+                                                      const int32_t* __restrict__ comp,
+                                                      const double* __restrict__ mass, const float* __restrict__ phi,
+                                                      double* __restrict__ part) {
+    __shared__ double red[8][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int k = blockIdx.y * 32 + tx;
+    const int s = src[k];
+    const int cs = s >= 0 ? comp[s] : -1;
+    const int v0 = blockIdx.x * kCompVTile;
+    const int v1 = min(n, v0 + kCompVTile);
+    double acc = 0.0;
+    for (int v = v0 + ty; v < v1; v += 8)
+        if (comp[v] == cs) acc = fma(mass[v], (double)phi[(int64_t)v * K + k], acc);
+    red[ty][tx] = acc;
+    __syncthreads();
+    if (ty == 0) {
+        double t = 0.0;
+        for (int j = 0; j < 8; ++j) t += red[j][tx];
+        part[(int64_t)blockIdx.x * K + k] = t;
+    }
+}
+
+// level[k] = sum over tiles of part[tile][k] / area of src[k]'s component, in a fixed order
+// (the same levels on every run).
+__global__ void __launch_bounds__(256) k_comp_mean(int32_t ntiles, int32_t K, const int32_t* __restrict__ src,
+                                                   const int32_t* __restrict__ comp,
+                                                   const double* __restrict__ area,
+                                                   const double* __restrict__ part, double* __restrict__ level) {
+    __shared__ double red[8][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int k = blockIdx.x * 32 + tx;
+    double acc = 0.0;
+    for (int t = ty; t < ntiles; t += 8) acc += part[(int64_t)t * K + k];
+    red[ty][tx] = acc;
+    __syncthreads();
+    if (ty == 0) {
+        double t = 0.0;
+        for (int j = 0; j < 8; ++j) t += red[j][tx];
+        const int s = src[k];
+        level[k] = s >= 0 ? t / area[comp[s]] : 0.0;
+    }
+}
+
+// phi[v][k] = level[k] for v off src[k]'s component
+__global__ void __launch_bounds__(256) k_comp_fill(int32_t n, int32_t K, const int32_t* __restrict__ src,
+                                                   const int32_t* __restrict__ comp,
+                                                   const double* __restrict__ level, float* __restrict__ phi) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int k = blockIdx.y * 32 + tx;
+    const int s = src[k];
+    if (s < 0) return;
+    const int cs = comp[s];
+    const float lv = (float)level[k];
+    const int v0 = blockIdx.x * kCompVTile;
+    const int v1 = min(n, v0 + kCompVTile);
+    for (int v = v0 + ty; v < v1; v += 8)
+        if (comp[v] != cs) phi[(int64_t)v * K + k] = lv;
+}
+
 }  // namespace
+
+int64_t component_tiles(int64_t n) { return (n + kCompVTile - 1) / kCompVTile; }
+
+void launch_component_level(const ComponentLevel& c, int32_t K, const int32_t* src, float* phi, double* scratch,
+                            cudaStream_t st) {
+    if (c.n <= 0 || K <= 0) return;
+    const int64_t nt = component_tiles(c.n);
+    double* level = scratch + nt * K;
+    const dim3 grid((unsigned)nt, (unsigned)(K / 32)), blk(32, 8);
+    k_comp_partial<<<grid, blk, 0, st>>>(c.n, K, src, c.comp, c.mass, phi, scratch);
+    k_comp_mean<<<K / 32, blk, 0, st>>>((int32_t)nt, K, src, c.comp, c.area, scratch, level);
+    k_comp_fill<<<grid, blk, 0, st>>>(c.n, K, src, c.comp, level, phi);
+}
 
 void launch_residual(const CsrOperator& A, int32_t K, const float* b, const float* x, float* r, cudaStream_t st) {
     if (A.n <= 0 || K <= 0) return;
