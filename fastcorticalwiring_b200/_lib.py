@@ -60,7 +60,7 @@ class FCWInfo(ctypes.Structure):
         ("analyze_ms", ctypes.c_double), ("factor_ms", ctypes.c_double), ("flops_factor", ctypes.c_double),
         ("device_bytes", ctypes.c_int64),
         ("pipeline_depth", ctypes.c_int32), ("block_k", ctypes.c_int32),
-        ("n_flips", ctypes.c_int64),
+        ("n_flips", ctypes.c_int64), ("n_components", ctypes.c_int64),
     ]
 
     def as_dict(self):

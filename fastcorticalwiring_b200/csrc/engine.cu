@@ -374,6 +374,33 @@ int validate_params(const fcw_params* p) {
     return FCW_OK;
 }
 
+// Connected components of the submesh (union-find over its faces; core_analysis.py:1349-1381
+// reports the same ones): comp[v] for each vertex v, numbered in order of first appearance in
+// the elimination order perm. Returns their count.
+int32_t mesh_components(const fcw::MeshPrep& m, const std::vector<int32_t>& perm, std::vector<int32_t>& comp) {
+    const int64_t n = m.nv;
+    std::vector<int32_t> up(n);
+    for (int64_t i = 0; i < n; ++i) up[i] = (int32_t)i;
+    auto find = [&](int32_t x) {
+        while (up[x] != x) x = up[x] = up[up[x]];
+        return x;
+    };
+    for (int64_t f = 0; f < m.nf; ++f)
+        for (int c = 1; c < 3; ++c) {
+            const int32_t a = find(m.F[3 * f]), b = find(m.F[3 * f + c]);
+            if (a != b) up[std::max(a, b)] = std::min(a, b);
+        }
+    std::vector<int32_t> label(n, -1);
+    comp.assign(n, -1);
+    int32_t count = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const int32_t v = perm[i], r = find(v);
+        if (label[r] < 0) label[r] = count++;
+        comp[v] = label[r];
+    }
+    return count;
+}
+
 // Values of A's lower entries in the symbolic analysis' order.
 enum class Op { Heat, Poisson, Grounded };
 std::vector<double> operator_values(const fcw_engine* e, Op op) {
@@ -421,44 +448,23 @@ int build_engine(fcw_engine* e, const double* V, int64_t nv, const int32_t* F, i
     const auto& m = e->mesh;
     if (S.max_ns > fcw::kMaxWidth) return fail(FCW_E_INVALID, "supernode wider than the kernels support");
     {
-        // connected components of the submesh (union-find over its faces), each grounded at its
-        // last eliminated vertex: L is singular once per component
-        std::vector<int32_t> up(S.n);
-        for (int64_t i = 0; i < S.n; ++i) up[i] = (int32_t)i;
-        auto find = [&](int32_t x) {
-            while (up[x] != x) x = up[x] = up[up[x]];
-            return x;
-        };
-        for (int64_t f = 0; f < m.nf; ++f)
-            for (int c = 1; c < 3; ++c) {
-                const int32_t a = find(m.F[3 * f]), b = find(m.F[3 * f + c]);
-                if (a != b) up[std::max(a, b)] = std::min(a, b);
-            }
-        std::vector<int32_t> last(S.n, -1);
-        for (int64_t i = 0; i < S.n; ++i) last[find(S.perm[i])] = (int32_t)i;  // ascending i: the last wins
+        // each connected component grounded at its last eliminated vertex: L is singular once
+        // per component
+        std::vector<int32_t> comp;
+        e->ncomp = mesh_components(m, S.perm, comp);
+        std::vector<int32_t> last(e->ncomp, -1);
+        for (int64_t i = 0; i < S.n; ++i) last[comp[S.perm[i]]] = (int32_t)i;  // ascending i: the last wins
         e->grounded_old.assign(S.n, 0);
-        e->ncomp = 0;
-        for (int64_t v = 0; v < S.n; ++v)
-            if (last[v] >= 0) {
-                e->grounded_old[S.perm[last[v]]] = 1;
-                ++e->ncomp;
-            }
+        for (int32_t c = 0; c < e->ncomp; ++c) e->grounded_old[S.perm[last[c]]] = 1;
         if (e->ncomp > 1) {
-            std::vector<int32_t> label(S.n, -1), comp(S.n);
-            std::vector<double> cmass(S.n), carea;
+            e->comp_h.resize(S.n);
+            e->cmass_h.resize(S.n);
+            e->carea_h.assign(e->ncomp, 0.0);
             for (int64_t i = 0; i < S.n; ++i) {
-                const int32_t r = find(S.perm[i]);
-                if (label[r] < 0) {
-                    label[r] = (int32_t)carea.size();
-                    carea.push_back(0.0);
-                }
-                comp[i] = label[r];
-                cmass[i] = m.mass[S.perm[i]];
-                carea[label[r]] += cmass[i];
+                e->comp_h[i] = comp[S.perm[i]];
+                e->cmass_h[i] = m.mass[S.perm[i]];
+                e->carea_h[e->comp_h[i]] += e->cmass_h[i];
             }
-            e->comp_h = std::move(comp);
-            e->cmass_h = std::move(cmass);
-            e->carea_h = std::move(carea);
         }
     }
 
@@ -1226,6 +1232,8 @@ int fcw_analyze(const double* V, int64_t nv, const int32_t* F, int64_t nf, const
         info->analyze_ms = now_ms() - t0;
         info->flops_factor = S.flops_factor;
         info->n_flips = nflips;
+        std::vector<int32_t> comp;
+        info->n_components = mesh_components(m, S.perm, comp);
     }
     if (perm_out) std::memcpy(perm_out, S.perm.data(), nv * sizeof(int32_t));
     return FCW_OK;
@@ -1309,6 +1317,7 @@ int fcw_engine_info(const fcw_engine* e, fcw_info* info) {
     info->pipeline_depth = (int32_t)e->pool.size();
     info->block_k = e->prm.block_k;
     info->n_flips = e->n_flips;
+    info->n_components = e->ncomp;
     return FCW_OK;
 }
 

@@ -288,6 +288,7 @@ class B200DistanceEngine(BaseDistanceEngine):
         info = self._engine.info()
         self.use_robust = robust
         self.n_flips = int(info["n_flips"])
+        self.n_components = int(info["n_components"])  # connected components of the submesh
         self.diffusion_length_mm = L
         self.mean_edge_length = float(info["mean_edge_length"])
         self.t_coef = float(info["t_coef"])

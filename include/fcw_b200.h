@@ -73,6 +73,7 @@ typedef struct fcw_info {
     int32_t pipeline_depth;     /* blocks in flight the device holds workspaces for (<= params) */
     int32_t block_k;            /* sources per block */
     int64_t n_flips;            /* intrinsic edge flips (robust operators; 0 otherwise) */
+    int64_t n_components;       /* connected components of the submesh (core_analysis.py:1349-1381) */
 } fcw_info;
 
 /* Per-source metric record: FCW_M_* offsets, then radii[nt], perimeters[nt],

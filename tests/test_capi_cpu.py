@@ -170,3 +170,26 @@ def test_refine_steps_are_validated():
     for bad in (-1, 5):
         with pytest.raises(_lib.FCWError):
             _lib.analyze(m.vertices, m.faces, refine=bad)
+
+
+def test_component_count_matches_scipy():
+    """fcw_info.n_components counts the submesh's connected components as the reference's
+    diagnostic does (core_analysis.py:1349-1381); the engine grounds one vertex of each."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import connected_components
+
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    a = folded_icosphere(3, seed=1, jitter=0.1)
+    b = folded_icosphere(2, seed=2, jitter=0.1)
+    c = folded_icosphere(2, seed=3, jitter=0.0)
+    parts = [a, b, c]
+    for k in (1, 2, 3):
+        V = np.vstack([p.vertices * (1.0 - 0.2 * i) for i, p in enumerate(parts[:k])])
+        offs = np.cumsum([0] + [len(p.vertices) for p in parts[:k]])
+        F = np.vstack([p.faces + offs[i] for i, p in enumerate(parts[:k])])
+        pm = M.prepare(V, F, np.concatenate([p.cortex_mask for p in parts[:k]]))
+        n = pm.n_vertices
+        G = sp.coo_matrix((np.ones(pm.F.size), (pm.F.ravel(), pm.F[:, [1, 2, 0]].ravel())), shape=(n, n))
+        info, _ = _lib.analyze(pm.V, pm.F)
+        assert info["n_components"] == connected_components(G, directed=False)[0] == k

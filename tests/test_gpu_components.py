@@ -55,6 +55,10 @@ def _check_against(d, ref, label, src, on_tol, off_tol):
         assert np.max(np.abs(d[j][~on] - ref[j][~on])) <= off_tol * scale, (j, "off")
 
 
+def test_engine_counts_the_components(two):
+    assert two["eng"].info()["n_components"] == 2
+
+
 def test_oracle_puts_other_components_at_the_mean_distance(two):
     for j, s in enumerate(two["src"]):
         on = two["label"] == two["label"][s]
