@@ -52,30 +52,38 @@ __global__ void k_add(int64_t n4, float4* __restrict__ y, const float4* __restri
     }
 }
 
-constexpr int kCompVTile = 256;
+constexpr int kCompVTile = 256;  // vertex rows per CTA: 8 warps x 32 rows
 
 // part[tile][k] = sum over the tile's vertices v in the component of src[k] of mass[v] phi[v][k].
-// 32 sources x 8 vertex rows per CTA: each warp reads 128 contiguous bytes of a row.
+// 64 sources per CTA: lane l holds columns 2l, 2l+1 (each warp reads 256 contiguous bytes of a
+// row), each warp 32 rows with four rows' loads in flight; the sums are taken in a fixed order.
 __global__ void __launch_bounds__(256) k_comp_partial(int32_t n, int32_t K, const int32_t* __restrict__ src,
                                                       const int32_t* __restrict__ comp,
                                                       const double* __restrict__ mass, const float* __restrict__ phi,
                                                       double* __restrict__ part) {
-    __shared__ double red[8][33];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int k = blockIdx.y * 32 + tx;
-    const int s = src[k];
-    const int cs = s >= 0 ? comp[s] : -1;
-    const int v0 = blockIdx.x * kCompVTile;
-    const int v1 = min(n, v0 + kCompVTile);
-    double acc = 0.0;
-    for (int v = v0 + ty; v < v1; v += 8)
-        if (comp[v] == cs) acc = fma(mass[v], (double)phi[(int64_t)v * K + k], acc);
-    red[ty][tx] = acc;
+    __shared__ double red[8][64];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int k = blockIdx.y * 64 + 2 * lane;
+    const int s0 = src[k], s1 = src[k + 1];
+    const int c0 = s0 >= 0 ? comp[s0] : -1, c1 = s1 >= 0 ? comp[s1] : -1;
+    const int v0 = blockIdx.x * kCompVTile + warp * 32;
+    const int v1 = min(n, v0 + 32);
+    double a0 = 0.0, a1 = 0.0;
+#pragma unroll 4
+    for (int v = v0; v < v1; ++v) {
+        const int cv = comp[v];
+        const double mv = mass[v];
+        const float2 p = *reinterpret_cast<const float2*>(phi + (int64_t)v * K + k);
+        if (cv == c0) a0 = fma(mv, (double)p.x, a0);
+        if (cv == c1) a1 = fma(mv, (double)p.y, a1);
+    }
+    red[warp][2 * lane] = a0;
+    red[warp][2 * lane + 1] = a1;
     __syncthreads();
-    if (ty == 0) {
+    if (threadIdx.x < 64) {
         double t = 0.0;
-        for (int j = 0; j < 8; ++j) t += red[j][tx];
-        part[(int64_t)blockIdx.x * K + k] = t;
+        for (int j = 0; j < 8; ++j) t += red[j][threadIdx.x];
+        part[(int64_t)blockIdx.x * K + blockIdx.y * 64 + threadIdx.x] = t;
     }
 }
 
@@ -100,20 +108,22 @@ __global__ void __launch_bounds__(256) k_comp_mean(int32_t ntiles, int32_t K, co
     }
 }
 
-// phi[v][k] = level[k] for v off src[k]'s component
+// phi[v][k] = level[k] for v off src[k]'s component (the layout of k_comp_partial)
 __global__ void __launch_bounds__(256) k_comp_fill(int32_t n, int32_t K, const int32_t* __restrict__ src,
                                                    const int32_t* __restrict__ comp,
                                                    const double* __restrict__ level, float* __restrict__ phi) {
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int k = blockIdx.y * 32 + tx;
-    const int s = src[k];
-    if (s < 0) return;
-    const int cs = comp[s];
-    const float lv = (float)level[k];
-    const int v0 = blockIdx.x * kCompVTile;
-    const int v1 = min(n, v0 + kCompVTile);
-    for (int v = v0 + ty; v < v1; v += 8)
-        if (comp[v] != cs) phi[(int64_t)v * K + k] = lv;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int k = blockIdx.y * 64 + 2 * lane;
+    const int s0 = src[k], s1 = src[k + 1];
+    const int c0 = s0 >= 0 ? comp[s0] : -1, c1 = s1 >= 0 ? comp[s1] : -1;
+    const float l0 = (float)level[k], l1 = (float)level[k + 1];
+    const int v0 = blockIdx.x * kCompVTile + warp * 32;
+    const int v1 = min(n, v0 + 32);
+    for (int v = v0; v < v1; ++v) {
+        const int cv = comp[v];
+        if (c0 >= 0 && cv != c0) phi[(int64_t)v * K + k] = l0;
+        if (c1 >= 0 && cv != c1) phi[(int64_t)v * K + k + 1] = l1;
+    }
 }
 
 }  // namespace
@@ -125,10 +135,10 @@ void launch_component_level(const ComponentLevel& c, int32_t K, const int32_t* s
     if (c.n <= 0 || K <= 0) return;
     const int64_t nt = component_tiles(c.n);
     double* level = scratch + nt * K;
-    const dim3 grid((unsigned)nt, (unsigned)(K / 32)), blk(32, 8);
-    k_comp_partial<<<grid, blk, 0, st>>>(c.n, K, src, c.comp, c.mass, phi, scratch);
-    k_comp_mean<<<K / 32, blk, 0, st>>>((int32_t)nt, K, src, c.comp, c.area, scratch, level);
-    k_comp_fill<<<grid, blk, 0, st>>>(c.n, K, src, c.comp, level, phi);
+    const dim3 grid((unsigned)nt, (unsigned)(K / 64));  // K is a multiple of 64
+    k_comp_partial<<<grid, 256, 0, st>>>(c.n, K, src, c.comp, c.mass, phi, scratch);
+    k_comp_mean<<<K / 32, dim3(32, 8), 0, st>>>((int32_t)nt, K, src, c.comp, c.area, scratch, level);
+    k_comp_fill<<<grid, 256, 0, st>>>(c.n, K, src, c.comp, level, phi);
 }
 
 void launch_residual(const CsrOperator& A, int32_t K, const float* b, const float* x, float* r, cudaStream_t st) {

@@ -102,3 +102,18 @@ def test_metrics_match_oracle(two, precision, tol):
         assert rel(r["radii"][j], ref["radii"]) <= tol
         assert rel(r["perim"][j], ref["perim"]) <= tol
         assert rel(r["msd_w"][j], ref["msd_w"]) <= tol
+
+
+@pytest.mark.parametrize("refine,robust", [(1, 0), (0, 1), (2, 1)])
+def test_refined_and_robust_mixed_match_fp64(two, refine, robust):
+    """The refinement residual and the intrinsic-Delaunay operators ground every component too."""
+    pm, src = two["pm"], two["src"]
+    eng = engine.HeatEngine(pm.V, pm.F, block_k=64, refine=refine, robust=robust)
+    try:
+        assert eng.info()["n_components"] == 2
+        d64 = eng.compute_distances(src, precision="fp64")
+        d32 = eng.compute_distances(src, precision="mixed")
+    finally:
+        eng.close()
+    assert np.all(np.isfinite(d32))
+    _check_against(d32, d64, two["label"], src, 1e-4, 1e-4)
