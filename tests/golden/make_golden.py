@@ -21,6 +21,9 @@ Fixtures:
   golden_metrics_L5.npz   same analysis outputs on a seeded folded L5 mesh (16 sources)
   golden_geometry_kat.npz lean geometry on euclid-stub and non-Lipschitz fields (L4 bumpy),
                           area/perimeter at fixed radii, per_source_geometry, NaN rules
+  golden_components_L4.npz the analysis on a submesh of two connected components (a seeded
+                          folded L4 mesh with a half-size folded L3 mesh inside it): fields and
+                          outputs for 10 sources in both components
   golden_samples_L5.npz   sample assembly with a boundary cap on the L5 mesh: 24 sources near
                           the boundary run through compute_all_wiring_costs(boundary_cap_fraction=0.05),
                           their FP64 geometry records and float32 distance to boundary, the sample
@@ -34,6 +37,7 @@ import io
 import os
 import sys
 import warnings
+from types import SimpleNamespace
 
 import numpy as np
 
@@ -324,12 +328,18 @@ def main():
         fx.pop("phi")  # large; the L5 fixture pins outputs, not fields
         return fx
 
+    a, b = folded_icosphere(4, seed=3, jitter=0.2), folded_icosphere(3, seed=5, jitter=0.1)
+    two = SimpleNamespace(vertices=np.vstack([a.vertices, 0.5 * b.vertices]),
+                          faces=np.vstack([a.faces, b.faces + len(a.vertices)]),
+                          cortex_mask=np.concatenate([a.cortex_mask, b.cortex_mask]), level=4, seed=3, jitter=0.2)
+
     fixtures = {
         "golden_heat_L4.npz": lambda: _analysis_fixture(ca, lg, fl, l4, 8, True),
         "golden_metrics_L5.npz": metrics_l5,
         "golden_geometry_kat.npz": lambda: _geometry_kat(ca, lg, tk),
         "golden_samples_L5.npz": lambda: _samples_fixture(ca, lg, l5, 24, 0.05),
         "golden_params_L4.npz": lambda: _params_fixture(ca, l4b, 12, 1.0, 1),
+        "golden_components_L4.npz": lambda: _analysis_fixture(ca, lg, fl, two, 10, False),
     }
     for name, make in fixtures.items():
         if args.only and name != args.only:

@@ -117,3 +117,31 @@ def test_refined_and_robust_mixed_match_fp64(two, refine, robust):
         eng.close()
     assert np.all(np.isfinite(d32))
     _check_against(d32, d64, two["label"], src, 1e-4, 1e-4)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-6), ("mixed", 1e-4)])
+def test_engine_matches_reference_outputs_on_two_components(precision, tol):
+    """The float32 arrays the reference's analysis wrote on a two-component submesh
+    (tests/golden/golden_components_L4.npz, made by the reference's own code)."""
+    import os
+
+    from tests.conftest import GOLDEN
+
+    z = dict(np.load(os.path.join(GOLDEN, "golden_components_L4.npz")))
+    pm = M.prepare(z["V"], z["F"], z["mask"])
+    eng = engine.HeatEngine(pm.V, pm.F, block_k=64)
+    try:
+        r = engine.split_records(eng.compute_metrics(z["sources_sub"].astype(np.int32), z["targets"], n_between=3,
+                                                     precision=precision), len(SCALES), 3)
+    finally:
+        eng.close()
+    rel = lambda a, b: np.abs(np.asarray(a, float) - b) / np.abs(b)  # noqa: E731
+    for j in range(z["sources_sub"].size):
+        assert bool(r["bad"][j]) == bool(z["field_flag"][j])
+        if r["bad"][j]:
+            continue
+        assert rel(r["msd_w"][j], z["f32_msd_weighted"][j]) <= max(tol, 2.4e-7)
+        for i, sc in enumerate(z["scales"]):
+            tok = format(float(sc), "g")
+            assert rel(r["radii"][j, i], z["f32_radius_" + tok][j]) <= max(tol, 2.4e-7)
+            assert rel(r["perim"][j, i], z["f32_perimeter_" + tok][j]) <= max(tol, 2.4e-7)

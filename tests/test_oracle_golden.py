@@ -112,6 +112,45 @@ def test_oracle_matches_reference_with_other_settings():
         assert hi - lo == len(z["scales"]) + (len(z["scales"]) - 1) * nb
 
 
+def test_oracle_matches_reference_on_two_components():
+    """A submesh of two connected components: the reference puts every vertex of the other
+    component at one level, the M-weighted mean distance over the source's component, which
+    carries the rounding of 1^T div X / shift (1e-9 of the field between two factorisations)."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    z = _load("golden_components_L4.npz")
+    pm = M.prepare(z["V"], z["F"], z["mask"])
+    assert np.array_equal(pm.bfs, z["bfs_order"])
+    n = pm.n_vertices
+    G = coo_matrix((np.ones(pm.F.size), (pm.F.ravel(), pm.F[:, [1, 2, 0]].ravel())), shape=(n, n))
+    ncomp, label = connected_components(G, directed=False)
+    assert ncomp == 2 and len(set(label[z["sources_sub"]])) == 2
+    ho = oracle.HeatOracle(pm.V, pm.F)
+    phi = ho.distances(z["sources_sub"])
+    mass = np.asarray(ho.mass).ravel()
+    for j, s in enumerate(z["sources_sub"]):
+        on = label == label[s]
+        ref = z["phi"][j]
+        scale = np.max(np.abs(ref))
+        assert np.max(np.abs(phi[j][on] - ref[on])) <= 1e-12 * scale
+        assert np.max(np.abs(phi[j][~on] - ref[~on])) <= 1e-8 * scale
+        assert np.ptp(ref[~on]) == 0.0
+        level = np.sum(mass[on] * ref[on]) / np.sum(mass[on])
+        assert abs(ref[~on][0] - level) <= 1e-8 * level
+        out = oracle.source_metrics(phi[j], int(s), pm, z["targets"])
+        assert out["bad"] == bool(z["field_flag"][j])
+        if out["bad"]:
+            assert np.isnan(z["f32_msd_weighted"][j])
+            continue
+        np.testing.assert_allclose(np.float32(out["msd_w"]), z["f32_msd_weighted"][j], rtol=2.4e-7)
+        np.testing.assert_allclose(np.float32(out["msd_u"]), z["f32_msd_unweighted"][j], rtol=2.4e-7)
+        for i, sc in enumerate(z["scales"]):
+            tok = format(float(sc), "g")
+            np.testing.assert_allclose(np.float32(out["radii"][i]), z["f32_radius_" + tok][j], rtol=2.4e-7)
+            np.testing.assert_allclose(np.float32(out["perim"][i]), z["f32_perimeter_" + tok][j], rtol=2.4e-7)
+
+
 def test_geometry_kat():
     z = _load("golden_geometry_kat.npz")
     V, F = z["V"], z["F"].astype(np.int32)
