@@ -139,7 +139,10 @@ int fcw_intrinsic_operators(const double* vertices, int64_t n_vertices, const in
  * M + tL and L + shift*M (and the grounded FP32 Poisson operator when
  * params->build_mixed). Replaces PotpourriDistanceEngine.__init__
  * (distance_engines.py:75-125) and ConsistentBatchHeatEngine.__init__
- * (fastcw_lean.py:481-502). */
+ * (fastcw_lean.py:481-502). The mesh may have several connected components
+ * (fcw_info.n_components): every field still spans all vertices, and the
+ * vertices off the source's component get the M-weighted mean distance over
+ * that component, in both precisions, as the FP64 operator gives them. */
 typedef struct fcw_engine fcw_engine;
 int fcw_engine_create(const double* vertices, int64_t n_vertices, const int32_t* faces, int64_t n_faces,
                       const fcw_params* params, fcw_engine** out);
