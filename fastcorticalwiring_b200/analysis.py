@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import json
 import os
+import time
 import warnings
 
 import numpy as np
@@ -166,18 +167,55 @@ class WiringAnalysis:
                                  boundary_cap_fraction=None, batch_size=None, verbose=False):
         """MSD, distance to boundary, radius, perimeter and (radius, area) samples of every source.
 
-        Arguments and validation follow core_analysis.py:1441-1500; area_tol, batch_size and
-        verbose are accepted and ignored as there.
+        Arguments and validation follow core_analysis.py:1441-1500; area_tol and batch_size are
+        accepted and ignored as there. The engine solves blocks of sources, so verbose prints one
+        timing line per block instead of one per source. Prints the end-of-run report and returns
+        ((msd_unweighted, msd_weighted), radius_function, perimeter_function), as
+        core_analysis.py:1634-1672 does.
         """
+        t0 = time.perf_counter()
         scales, m, cap = self.run_arguments(scale, n_samples_between_scales, boundary_cap_fraction)
         targets = self._reset(scales, m, cap)
         order = self._sources(vertex_subset)
         eng = self.distance_engine.engine
         for b0 in range(0, order.size, self.block_sources):
+            tb = time.perf_counter()
             sub = order[b0:b0 + self.block_sources]
             rec = eng.compute_metrics(sub, targets, n_between=m, eps=self.eps, precision=self.precision)
             self._absorb(sub, rec, eng.assemble_samples(rec, targets, n_between=m, boundary_cap=cap))
-        self._finish(order.size)
+            if verbose:
+                print(f"[{b0 + sub.size}/{order.size}] block of {sub.size} sources: "
+                      f"{1e3 * (time.perf_counter() - tb):.2f}ms")
+        flagged = self._finish(order.size)
+        self.report(order.size, flagged, time.perf_counter() - t0)
+        return (self.msd_unweighted, self.msd_weighted), self.radius_function, self.perimeter_function
+
+    def report(self, n_sources, flagged, seconds):
+        """The end-of-run printout of core_analysis.py:1634-1670: the flagged fields (the first ten
+        with their health fractions), the run time, and min/max/mean of MSD, radius and perimeter."""
+        if flagged:
+            print(f"WARNING: {len(flagged)} of {n_sources} source vertices had corrupted distance fields; "
+                  "all metrics for them were set to NaN (see field_flag).")
+            for orig_idx, neg, viol in flagged[:10]:
+                print(f"  vertex {orig_idx}: negative fraction {neg:.4f}, chord-violation fraction {viol:.4f}")
+        if n_sources > 0:
+            print(f"Timing over {n_sources} vertices: {seconds:.1f}s ({1e3 * seconds / n_sources:.3f} ms/vertex) "
+                  f"on the {getattr(self.distance_engine, 'name', 'b200')} engine, {self.precision}")
+
+        def stats(prefix, values):
+            v = values[np.isfinite(values)]
+            if v.size:
+                print(f"{prefix}min={np.min(v):.2f}, max={np.max(v):.2f}, mean={np.mean(v):.2f}")
+
+        if np.isfinite(self.msd_unweighted).any():
+            print("MSD (unweighted, Ecker 2013 definition):")
+            stats("  ", self.msd_unweighted)
+        if np.isfinite(self.msd_weighted).any():
+            print("MSD (area-weighted, resampling-invariant):")
+            stats("  ", self.msd_weighted)
+        for s in self.active_scales:
+            stats(f"Radius stats @ {s * 100:.2f}%: ", self.radius_function[float(s)])
+            stats(f"Perimeter stats @ {s * 100:.2f}%: ", self.perimeter_function[float(s)])
 
     @classmethod
     def run_arguments(cls, scale, n_samples_between_scales, boundary_cap_fraction):
@@ -261,6 +299,7 @@ class WiringAnalysis:
             msg = (f"{len(flagged)} of {n_sources} source vertices had corrupted distance fields; "
                    "all metrics for them were set to NaN (see field_flag).")
             warnings.warn(msg, RuntimeWarning)
+        return flagged
 
     # -- results -------------------------------------------------------------
     def provenance(self):

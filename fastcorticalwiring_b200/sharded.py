@@ -17,6 +17,7 @@ subject's sources over several GPUs.
 from __future__ import annotations
 
 import os
+import time
 
 import numpy as np
 
@@ -88,7 +89,9 @@ class ShardedWiringAnalysis(WiringAnalysis):
     def compute_all_wiring_costs(self, scale=None, area_tol=None, vertex_subset=None, n_samples_between_scales=3,
                                  boundary_cap_fraction=None, batch_size=None, verbose=False):
         """As WiringAnalysis.compute_all_wiring_costs (core_analysis.py:1441-1672), with each rank
-        computing its slice of the sources and the records gathered to every rank."""
+        computing its slice of the sources and the records gathered to every rank. Every rank
+        returns the same arrays; rank 0 prints the end-of-run report."""
+        t0 = time.perf_counter()
         scales, m, cap = self.run_arguments(scale, n_samples_between_scales, boundary_cap_fraction)
         targets = self._reset(scales, m, cap)
         order = self._sources(vertex_subset)
@@ -103,4 +106,7 @@ class ShardedWiringAnalysis(WiringAnalysis):
         rec = gather_rows(local, self.group)
         if order.size:
             self._absorb(order, rec, eng.assemble_samples(rec, targets, n_between=m, boundary_cap=cap))
-        self._finish(order.size)
+        flagged = self._finish(order.size)
+        if rank == 0:
+            self.report(order.size, flagged, time.perf_counter() - t0)
+        return (self.msd_unweighted, self.msd_weighted), self.radius_function, self.perimeter_function

@@ -141,3 +141,31 @@ def test_shard_slices():
 
     with pytest.raises(ValueError):
         sharded.shard(order, 2, 2)
+
+
+def test_run_returns_the_reference_tuple_and_prints_its_report(capsys):
+    """compute_all_wiring_costs returns ((msd_unweighted, msd_weighted), radius_function,
+    perimeter_function) and prints the end-of-run report, as core_analysis.py:1634-1672 does;
+    verbose prints one line per block of sources."""
+    import warnings
+
+    from fastcorticalwiring_b200 import analysis
+
+    analysis.B200DistanceEngine = _StandInDistanceEngine
+    a = analysis.WiringAnalysis(*_mesh(), block_sources=64)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        (msd_u, msd_w), radius, perim = a.compute_all_wiring_costs(scale=list(SCALES), n_samples_between_scales=2,
+                                                                    verbose=True)
+    assert msd_u is a.msd_unweighted and msd_w is a.msd_weighted
+    assert radius is a.radius_function and perim is a.perimeter_function
+    out = capsys.readouterr().out.splitlines()
+    assert any(line.startswith("[64/") for line in out)
+    assert any(line.startswith(f"WARNING: {a.n_flagged_fields} of ") for line in out)
+    assert sum(line.startswith("  vertex ") for line in out) == min(10, a.n_flagged_fields)
+    assert "MSD (unweighted, Ecker 2013 definition):" in out
+    v = msd_u[np.isfinite(msd_u)]
+    assert f"  min={v.min():.2f}, max={v.max():.2f}, mean={v.mean():.2f}" in out
+    for s in SCALES:
+        assert any(line.startswith(f"Radius stats @ {s * 100:.2f}%: min=") for line in out)
+        assert any(line.startswith(f"Perimeter stats @ {s * 100:.2f}%: min=") for line in out)
