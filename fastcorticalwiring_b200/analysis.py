@@ -50,6 +50,28 @@ def classify_nonmanifold_vertices(vertices, faces):
             "also_boundary": non_manifold & boundary, "interior": non_manifold - boundary}
 
 
+def report_components(pm):
+    """Print the cortical submesh's connected components, as the reference's analysis does at
+    construction (core_analysis.py:1349-1381); returns their sizes, largest first. Every source
+    still yields a field over the whole submesh."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    n = pm.n_vertices
+    if n == 0:
+        print("Connected components in cortical submesh: 0")
+        return np.zeros(0, dtype=np.int64)
+    F = np.asarray(pm.F)
+    G = coo_matrix((np.ones(F.size, dtype=np.uint8), (F.ravel(), F[:, [1, 2, 0]].ravel())), shape=(n, n))
+    ncomp, label = connected_components(G, directed=False)
+    sizes = np.sort(np.bincount(label, minlength=ncomp))[::-1]
+    print(f"Connected components in cortical submesh: {int(ncomp)}")
+    if ncomp > 1:
+        more = " ..." if ncomp > 20 else ""
+        print("Component sizes: " + ", ".join(str(int(x)) for x in sizes[:20]) + more)
+    return sizes
+
+
 def check_interior_nonmanifold(pm, engine_type="b200", allow=False):
     """Count the cortical submesh's interior non-manifold vertices and warn about them unless
     allowed, as the reference does for engines without the robust fallback
@@ -90,6 +112,7 @@ class WiringAnalysis:
         pm = self.mesh
         self.n_interior_nonmanifold = check_interior_nonmanifold(pm, self.engine_type,
                                                                  self.allow_interior_nonmanifold)
+        self.component_sizes = report_components(pm)
         self.distance_engine = B200DistanceEngine(pm.V, pm.F, **dict(engine_kwargs or {}))
         self.eps = float(eps)
         self.precision = precision

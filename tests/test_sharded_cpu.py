@@ -169,3 +169,20 @@ def test_run_returns_the_reference_tuple_and_prints_its_report(capsys):
     for s in SCALES:
         assert any(line.startswith(f"Radius stats @ {s * 100:.2f}%: min=") for line in out)
         assert any(line.startswith(f"Perimeter stats @ {s * 100:.2f}%: min=") for line in out)
+
+
+def test_construction_reports_the_components(capsys):
+    """The constructor prints the submesh's connected components (core_analysis.py:1349-1381)."""
+    from fastcorticalwiring_b200 import analysis
+
+    analysis.B200DistanceEngine = _StandInDistanceEngine
+    a = folded_icosphere(3, seed=2, jitter=0.1)
+    b = folded_icosphere(2, seed=4, jitter=0.0)
+    V = np.vstack([a.vertices, 0.5 * b.vertices])
+    F = np.vstack([a.faces, b.faces + len(a.vertices)])
+    an = analysis.WiringAnalysis(V, F, np.concatenate([a.cortex_mask, b.cortex_mask]))
+    out = capsys.readouterr().out.splitlines()
+    assert "Connected components in cortical submesh: 2" in out
+    sizes = an.component_sizes
+    assert sizes.size == 2 and sizes.sum() == an.mesh.n_vertices
+    assert f"Component sizes: {sizes[0]}, {sizes[1]}" in out
