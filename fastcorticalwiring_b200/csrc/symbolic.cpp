@@ -5,6 +5,7 @@
 // principal axis, two directions orthogonal to it and their mixes), the one
 // whose smaller one-sided boundary between the halves is smallest; that boundary
 // becomes the vertex separator, numbered after both halves. Sets of at most `leaf_size` vertices are leaves.
+// The halves of the top three splits are dissected on their own threads; the order is the serial one.
 // The elimination tree is then postordered (same fill, contiguous subtrees),
 // and columns are grouped into supernodes:
 //   * relaxed supernodes: every maximal subtree of at most `relax` columns
@@ -15,8 +16,12 @@
 // its parent, per-row segments for the forward pull, the supernodal etree
 // levels, and where each lower entry of A lands in the panel storage.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <memory>
 #include <numeric>
+#include <system_error>
+#include <thread>
 
 #include "fcw_internal.h"
 
@@ -109,16 +114,28 @@ void candidate_axes(const double a[3], double dirs[kCandidates][3]) {
     }
 }
 
+// The two halves of a split are dissected on separate threads down to kParallelDepth
+// (disjoint vertex sets and output ranges). Each call marks its vertex set with a fresh
+// id; a neighbour's mark is read across the cut while another thread may rewrite it, so
+// the marks are relaxed atomics. A foreign mark never equals the reader's fresh id, and
+// side[] is read only for vertices of the reader's own set, so the order is the same as
+// a serial run's.
+constexpr int kParallelDepth = 3;
+constexpr int64_t kParallelMin = 4096;  // smaller sets stay on the calling thread
+
 struct Dissector {
     const Graph& g;
     const double* X;
     int leaf;
-    std::vector<int32_t> stamp;
+    std::unique_ptr<std::atomic<int32_t>[]> stamp;
     std::vector<int8_t> side;
-    int32_t next_id = 1;
+    std::atomic<int32_t> next_id{1};
 
     Dissector(const Graph& g_, const double* X_, int leaf_)
-        : g(g_), X(X_), leaf(leaf_), stamp(g_.n, 0), side(g_.n, 0) {}
+        : g(g_), X(X_), leaf(leaf_), stamp(new std::atomic<int32_t>[g_.n]), side(g_.n, 0) {
+        for (int64_t i = 0; i < g_.n; ++i) stamp[i].store(0, std::memory_order_relaxed);
+    }
+    bool member(int32_t y, int32_t id) const { return stamp[y].load(std::memory_order_relaxed) == id; }
 
     // Size of the smaller one-sided boundary of the median split of proj (-1 if one side is empty).
     int64_t separator_size(const int32_t* v, int64_t n, const std::vector<double>& proj, double med, int32_t id) {
@@ -133,7 +150,7 @@ struct Dissector {
             const int32_t x = v[i];
             for (int64_t k = g.xadj[x]; k < g.xadj[x + 1]; ++k) {
                 const int32_t y = g.adj[k];
-                if (stamp[y] == id && side[y] != side[x]) {
+                if (member(y, id) && side[y] != side[x]) {
                     (side[x] == 0 ? s0 : s1)++;
                     break;
                 }
@@ -143,13 +160,13 @@ struct Dissector {
     }
 
     // Writes an elimination order of v[0..n) into out[0..n).
-    void dissect(const int32_t* v, int64_t n, int32_t* out) {
+    void dissect(const int32_t* v, int64_t n, int32_t* out, int depth = 0) {
         if (n <= leaf) {
             std::copy(v, v + n, out);
             return;
         }
-        int32_t id = next_id++;
-        for (int64_t i = 0; i < n; ++i) stamp[v[i]] = id;
+        const int32_t id = next_id.fetch_add(1, std::memory_order_relaxed);
+        for (int64_t i = 0; i < n; ++i) stamp[v[i]].store(id, std::memory_order_relaxed);
         double c[3], ax[3];
         principal_axis(X, v, n, c, ax);
         // candidate cut directions: the principal axis, two directions orthogonal to it, and
@@ -196,7 +213,7 @@ struct Dissector {
             int32_t x = v[i];
             for (int64_t k = g.xadj[x]; k < g.xadj[x + 1]; ++k) {
                 int32_t y = g.adj[k];
-                if (stamp[y] == id && side[y] != side[x]) {
+                if (member(y, id) && side[y] != side[x]) {
                     (side[x] == 0 ? b0 : b1).push_back(x);
                     break;
                 }
@@ -212,8 +229,20 @@ struct Dissector {
             else if (side[v[i]] == 1) B.push_back(v[i]);
         }
         std::vector<int32_t> S(sep);
-        dissect(A.data(), (int64_t)A.size(), out);
-        dissect(B.data(), (int64_t)B.size(), out + A.size());
+        std::thread t;
+        if (depth < kParallelDepth && (int64_t)std::min(A.size(), B.size()) >= kParallelMin) {
+            try {
+                t = std::thread([&] { dissect(A.data(), (int64_t)A.size(), out, depth + 1); });
+            } catch (const std::system_error&) {  // no thread to be had: stay serial
+            }
+        }
+        if (t.joinable()) {
+            dissect(B.data(), (int64_t)B.size(), out + A.size(), depth + 1);
+            t.join();
+        } else {
+            dissect(A.data(), (int64_t)A.size(), out, depth + 1);
+            dissect(B.data(), (int64_t)B.size(), out + A.size(), depth + 1);
+        }
         std::copy(S.begin(), S.end(), out + A.size() + B.size());
     }
 };

@@ -193,3 +193,18 @@ def test_component_count_matches_scipy():
         G = sp.coo_matrix((np.ones(pm.F.size), (pm.F.ravel(), pm.F[:, [1, 2, 0]].ravel())), shape=(n, n))
         info, _ = _lib.analyze(pm.V, pm.F)
         assert info["n_components"] == connected_components(G, directed=False)[0] == k
+
+
+def test_elimination_order_is_deterministic():
+    """The nested dissection runs the halves of its top splits on separate threads; the order
+    (and so the factor's structure) must not depend on their timing."""
+    from fastcorticalwiring_b200.meshgen import folded_icosphere
+
+    m = folded_icosphere(6, seed=3, jitter=0.2)
+    pm = M.prepare(m.vertices, m.faces, m.cortex_mask)
+    info0, perm0 = _lib.analyze(pm.V, pm.F)
+    assert sorted(perm0.tolist()) == list(range(pm.n_vertices))
+    for _ in range(4):
+        info, perm = _lib.analyze(pm.V, pm.F)
+        assert np.array_equal(perm, perm0)
+        assert info["nnz_factor"] == info0["nnz_factor"] and info["n_supernodes"] == info0["n_supernodes"]
