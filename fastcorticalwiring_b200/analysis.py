@@ -50,21 +50,24 @@ def classify_nonmanifold_vertices(vertices, faces):
             "also_boundary": non_manifold & boundary, "interior": non_manifold - boundary}
 
 
-def report_components(pm):
+def report_components(pm, quiet=False):
     """Print the cortical submesh's connected components, as the reference's analysis does at
-    construction (core_analysis.py:1349-1381); returns their sizes, largest first. Every source
-    still yields a field over the whole submesh."""
+    construction (core_analysis.py:1349-1381), unless quiet; returns their sizes, largest
+    first. Every source still yields a field over the whole submesh."""
     from scipy.sparse import coo_matrix
     from scipy.sparse.csgraph import connected_components
 
     n = pm.n_vertices
     if n == 0:
-        print("Connected components in cortical submesh: 0")
+        if not quiet:
+            print("Connected components in cortical submesh: 0")
         return np.zeros(0, dtype=np.int64)
     F = np.asarray(pm.F)
     G = coo_matrix((np.ones(F.size, dtype=np.uint8), (F.ravel(), F[:, [1, 2, 0]].ravel())), shape=(n, n))
     ncomp, label = connected_components(G, directed=False)
     sizes = np.sort(np.bincount(label, minlength=ncomp))[::-1]
+    if quiet:
+        return sizes
     print(f"Connected components in cortical submesh: {int(ncomp)}")
     if ncomp > 1:
         more = " ..." if ncomp > 20 else ""
@@ -112,7 +115,8 @@ class WiringAnalysis:
         pm = self.mesh
         self.n_interior_nonmanifold = check_interior_nonmanifold(pm, self.engine_type,
                                                                  self.allow_interior_nonmanifold)
-        self.component_sizes = report_components(pm)
+        self.quiet = getattr(self, "quiet", False)  # no printed reports (a subclass may set it first)
+        self.component_sizes = report_components(pm, quiet=self.quiet)
         self.distance_engine = B200DistanceEngine(pm.V, pm.F, **dict(engine_kwargs or {}))
         self.eps = float(eps)
         self.precision = precision
@@ -216,6 +220,8 @@ class WiringAnalysis:
     def report(self, n_sources, flagged, seconds):
         """The end-of-run printout of core_analysis.py:1634-1670: the flagged fields (the first ten
         with their health fractions), the run time, and min/max/mean of MSD, radius and perimeter."""
+        if self.quiet:
+            return
         if flagged:
             print(f"WARNING: {len(flagged)} of {n_sources} source vertices had corrupted distance fields; "
                   "all metrics for them were set to NaN (see field_flag).")

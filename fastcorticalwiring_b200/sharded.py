@@ -84,6 +84,7 @@ class ShardedWiringAnalysis(WiringAnalysis):
         kw = dict(engine_kwargs or {})
         kw.setdefault("device", int(os.environ.get("LOCAL_RANK", "0")))
         self.group = group
+        self.quiet = _group_info(group)[0] != 0  # rank 0 alone prints the run's reports
         super().__init__(vertices, faces, cortex_mask, engine_type=engine_type, engine_kwargs=kw, **kwargs)
 
     def compute_all_wiring_costs(self, scale=None, area_tol=None, vertex_subset=None, n_samples_between_scales=3,
@@ -107,6 +108,5 @@ class ShardedWiringAnalysis(WiringAnalysis):
         if order.size:
             self._absorb(order, rec, eng.assemble_samples(rec, targets, n_between=m, boundary_cap=cap))
         flagged = self._finish(order.size)
-        if rank == 0:
-            self.report(order.size, flagged, time.perf_counter() - t0)
+        self.report(order.size, flagged, time.perf_counter() - t0)
         return (self.msd_unweighted, self.msd_weighted), self.radius_function, self.perimeter_function
