@@ -67,36 +67,47 @@ int prepare_mesh(const double* V, int64_t nv, const int32_t* F, int64_t nf, Mesh
     m.V.assign(V, V + 3 * nv);
     m.F.assign(F, F + 3 * nf);
 
-    // Unique undirected edges, sorted (distance_engines.py:17-21).
-    std::vector<int64_t> ekey;
-    ekey.reserve(3 * nf);
-    std::vector<int32_t> deg_on_edge;
-    for (int64_t f = 0; f < nf; ++f) {
-        for (int c = 0; c < 3; ++c) {
-            int64_t a = F[3 * f + c], b = F[3 * f + (c + 1) % 3];
-            if (a > b) std::swap(a, b);
-            ekey.push_back(a * nv + b);
-        }
-    }
-    std::sort(ekey.begin(), ekey.end());
+    // Unique undirected edges (a < b) in ascending (a, b) order, the order of the reference's
+    // sorted unique edge list (distance_engines.py:17-21): bucketed by a, each bucket's b
+    // sorted; the mean edge length sums them in that order. Free edges (one face) give the
+    // boundary vertices (core_analysis.py:651-665).
     {
+        std::vector<int64_t> eptr(nv + 1, 0);
+        for (int64_t f = 0; f < nf; ++f)
+            for (int c = 0; c < 3; ++c) eptr[std::min(F[3 * f + c], F[3 * f + (c + 1) % 3]) + 1]++;
+        for (int64_t v = 0; v < nv; ++v) eptr[v + 1] += eptr[v];
+        std::vector<int32_t> eb(3 * nf);
+        {
+            std::vector<int64_t> fill(eptr.begin(), eptr.end() - 1);
+            for (int64_t f = 0; f < nf; ++f)
+                for (int c = 0; c < 3; ++c) {
+                    const int32_t a = F[3 * f + c], b = F[3 * f + (c + 1) % 3];
+                    eb[fill[std::min(a, b)]++] = std::max(a, b);
+                }
+        }
         double sum = 0.0;
         int64_t cnt = 0;
         std::vector<int32_t> bverts;
-        for (size_t i = 0; i < ekey.size();) {
-            size_t j = i;
-            while (j < ekey.size() && ekey[j] == ekey[i]) ++j;
-            int64_t a = ekey[i] / nv, b = ekey[i] % nv;
-            double d[3] = {V[3 * b] - V[3 * a], V[3 * b + 1] - V[3 * a + 1], V[3 * b + 2] - V[3 * a + 2]};
-            sum += norm3(d);
-            ++cnt;
-            if (j - i == 1) { bverts.push_back((int32_t)a); bverts.push_back((int32_t)b); }  // free edge
-            i = j;
+        for (int64_t a = 0; a < nv; ++a) {
+            int32_t* lo = eb.data() + eptr[a];
+            int32_t* hi = eb.data() + eptr[a + 1];
+            for (int32_t* p = lo + 1; p < hi; ++p)  // insertion sort: a handful of entries
+                for (int32_t* q = p; q > lo && q[-1] > q[0]; --q) std::swap(q[-1], q[0]);
+            for (int32_t* p = lo; p < hi;) {
+                int32_t* r = p;
+                while (r < hi && *r == *p) ++r;
+                const int64_t b = *p;
+                double d[3] = {V[3 * b] - V[3 * a], V[3 * b + 1] - V[3 * a + 1], V[3 * b + 2] - V[3 * a + 2]};
+                sum += norm3(d);
+                ++cnt;
+                if (r - p == 1) { bverts.push_back((int32_t)a); bverts.push_back((int32_t)b); }  // free edge
+                p = r;
+            }
         }
         m.mean_edge = sum / (double)cnt;
         std::sort(bverts.begin(), bverts.end());
         bverts.erase(std::unique(bverts.begin(), bverts.end()), bverts.end());
-        m.boundary = bverts;  // core_analysis.py:651-665
+        m.boundary = bverts;
     }
 
     // Face max edge, bucket width and health length (lean_geometry.py:99-114, core_analysis.py:705, 913-957).
@@ -190,8 +201,12 @@ int prepare_mesh(const double* V, int64_t nv, const int32_t* F, int64_t nf, Mesh
                     ent.push_back({F[3 * f + i], (int64_t)(3 * i + j) * nf + f,
                                    m.grad_area[f] * einsum_dot3(g + 3 * i, g + 3 * j)});
             }
-            std::sort(ent.begin(), ent.end(),
-                      [](const Entry& a, const Entry& b) { return a.row != b.row ? a.row < b.row : a.pos < b.pos; });
+            // (row, pos) keys are distinct, so this insertion sort (a few dozen entries) gives
+            // the one sorted order
+            for (size_t k = 1; k < ent.size(); ++k)
+                for (size_t q = k; q > 0 && (ent[q - 1].row != ent[q].row ? ent[q - 1].row > ent[q].row
+                                                                         : ent[q - 1].pos > ent[q].pos); --q)
+                    std::swap(ent[q - 1], ent[q]);
             for (size_t k = 0; k < ent.size();) {
                 size_t l = k;
                 double sum = 0.0;
