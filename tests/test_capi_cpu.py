@@ -193,6 +193,8 @@ def test_component_count_matches_scipy():
         G = sp.coo_matrix((np.ones(pm.F.size), (pm.F.ravel(), pm.F[:, [1, 2, 0]].ravel())), shape=(n, n))
         info, _ = _lib.analyze(pm.V, pm.F)
         assert info["n_components"] == connected_components(G, directed=False)[0] == k
+        # the intrinsic edge flips stay inside a component
+        assert _lib.analyze(pm.V, pm.F, robust=1)[0]["n_components"] == k
 
 
 def test_elimination_order_is_deterministic():
